@@ -1,0 +1,347 @@
+"""Benchmark of the sm_100a mPDeC5 time step (one JSON line on rank 0).
+
+Workload: the wave-over-dry-island case on a 2048x2048 periodic grid ([0,10]^2,
+Gaussian island b = 1.2 exp(-((x-5)^2+(y-5)^2)/0.5), still water h + b = 1 with
+a hump of amplitude 0.3 and width 0.3 at x = 2), CFL 0.4, g = 9.81.  A step is
+TimeStep() + one mPDeC5 step (13 RHS evaluations, 13 Patankar solves).
+
+  value        split-precision cell-steps/s with the state resident in HBM
+  fp64         the plain FP64 form on the same workload (the metric's baseline)
+  e2e          the same metric through the C ABI with host buffers: every step
+               copies the ghosted state host->device and back (swm_set_state /
+               swm_get_state), as a Fortran driver keeping U on the host would
+  roofline     dominant kernel, algorithmic bytes / CUDA-event time
+  cpu_baseline the CPU restatement (oracle, OpenMP build) on a bounded sample
+
+Multi-GPU (--gpus N under torchrun): replicas only -- every rank steps its own
+copy of the workload on its GPU, no data-path collective; value = N * cells *
+steps / (max over ranks of the timed region).
+
+--impl reference times the reference's CPU path (the oracle restatement: the
+Fortran reference cannot be compiled in this image) on a bounded sample of the
+same workload with all host threads.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "sw-mpdec_b200"))
+
+METRIC = "mPDeC5 cell-steps/s at 2048²: split-precision vs FP64 GPU at L1 err ≤1e-6"
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d, "measured"
+    return PEAKS_FALLBACK, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if parts[3 + k].lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_solver(swm, c, precision, solver="stencil", block=4, device=0):
+    return swm.Solver(nx=c["nx"], ny=c["ny"], x0=c["x0"], x1=c["x1"], g=c["g"], cfl=c["cfl"],
+                      bathy_flag=c["bathy_flag"], bathy_par=c["bathy_par"],
+                      well_balanced=c["well_balanced"], precision=precision, solver=solver,
+                      jacobi_block=block, device=device)
+
+
+def timed_steps(s, torch, steps, warmup):
+    """W untimed steps, then K steps bracketed by CUDA events on the library stream."""
+    for _ in range(warmup):
+        s.step(0.0, s.timestep())
+    st = torch.cuda.ExternalStream(s.stream())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(st)
+    iters = 0
+    for _ in range(steps):
+        s.step(0.0, s.timestep())
+        iters += sum(s.stats()["jacobi_iters"])
+    e1.record(st)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1), iters
+
+
+def cpu_sample(steps=1, n=512):
+    """Oracle (OpenMP build) on the island case at n^2 (same domain and physics)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import cases
+    import oracle as O
+    c = cases.case("island", n=n)
+    p = O.make_params(c["nx"], c["ny"], c["x0"], c["x1"], g=c["g"], cfl=c["cfl"],
+                      bathy_flag=c["bathy_flag"], bathy_par=c["bathy_par"])
+    o = O.Oracle(p, threaded=True)
+    o.set_planes(cases.cell_averages(c))
+    dt = o.timestep()
+    o.step(0.0, dt)  # warm-up (page-in)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        o.step(0.0, o.timestep())
+    el = time.perf_counter() - t0
+    return {"value": c["nx"] * c["ny"] * steps / el, "unit": "cell-steps/s",
+            "cores": O.threads(True), "kind": "port",
+            "sample": f"island case at {n}x{n} (same domain/physics), {steps} mPDeC5 step(s) "
+                      f"after 1 warm-up, CPU restatement of the Fortran (oracle/swm_oracle.c, "
+                      f"OpenMP build)"}
+
+
+def reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+    n = 512
+    warm = max(args.warmup, 0)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import cases
+    import oracle as O
+    c = cases.case("island", n=n)
+    p = O.make_params(c["nx"], c["ny"], c["x0"], c["x1"], g=c["g"], cfl=c["cfl"],
+                      bathy_flag=c["bathy_flag"], bathy_par=c["bathy_par"])
+    o = O.Oracle(p, threaded=True)
+    o.set_planes(cases.cell_averages(c))
+    for _ in range(warm):
+        o.step(0.0, o.timestep())
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        o.step(0.0, o.timestep())
+    el = time.perf_counter() - t0
+    v = c["nx"] * c["ny"] * args.steps / el
+    cores = O.threads(True)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "cell-steps/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"island {n}x{n} sample of the 2048x2048 wave-over-dry-island "
+                               f"case (same domain, bathymetry and hump), mPDeC5, CFL 0.4",
+                   "parallelism": "host threads"},
+        "cpu_baseline": {"value": v, "unit": "cell-steps/s", "cores": cores, "kind": "port",
+                         "sample": f"{args.steps} mPDeC5 steps of the island case at {n}x{n} "
+                                   f"after {warm} warm-up steps; the Fortran reference has no "
+                                   f"compiler here, so its C restatement (oracle) is timed"},
+        "e2e": {"value": v, "unit": "cell-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="swm")
+    ap.add_argument("--block", type=int, default=4)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--n", type=int, default=2048)
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if args.impl == "reference":
+        reference_arm(args, rank, world)
+        return
+
+    import torch
+    import swm
+    import cases
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    c = cases.case("island", n=args.n)
+    cells = c["nx"] * c["ny"]
+    planes = cases.cell_averages(c)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    results = {}
+    clocks = None
+    for prec in ("fp64", "split"):
+        s = make_solver(swm, c, prec, block=args.block, device=local)
+        s.set_planes(planes)
+        barrier()
+        sampler = ClockSampler(local) if prec == "split" else None
+        if sampler:
+            sampler.start()
+        ms, iters = timed_steps(s, torch, args.steps, args.warmup)
+        if sampler:
+            clocks = sampler.stop()
+        barrier()
+        ms = max_over_ranks(ms)
+        prof = s.profile_step(0.0, s.timestep())  # one extra eagerly-launched step
+        results[prec] = dict(ms=ms, iters=iters, prof=prof, final=s.get_planes())
+        s.close()
+        del s
+
+    # accuracy of the split form against the FP64 form on the same steps
+    a, b = results["split"]["final"], results["fp64"]["final"]
+    l1 = [float(np.abs(a[v] - b[v]).sum() / max(np.abs(b[v]).sum(), 1e-300)) for v in range(3)]
+    hmin = float(a[0].min())
+
+    # end to end through the C ABI with host buffers
+    e2e = None
+    if not args.no_e2e:
+        s = make_solver(swm, c, "split", block=args.block, device=local)
+        Ug = torch.from_numpy(cases.ghosted(planes)).pin_memory().numpy()
+        Uo = torch.empty(Ug.shape, dtype=torch.float64).pin_memory().numpy()
+        s.set_state(Ug)
+        for _ in range(args.warmup):
+            s.set_state(Ug)
+            s.step(0.0, s.timestep())
+            s.get_state()
+        barrier()
+        st = torch.cuda.ExternalStream(s.stream())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(args.steps):
+            s.set_state(Ug)
+            s.step(0.0, s.timestep())
+            s.lib.swm_get_state(s.h, swm._dp(Uo), None)
+        e1.record(st)
+        torch.cuda.synchronize()
+        ms_e2e = max_over_ranks(e0.elapsed_time(e1))
+        nbytes = Ug.nbytes
+        e2e = {"value": world * cells * args.steps / (ms_e2e * 1e-3), "unit": "cell-steps/s",
+               "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes + 16,
+               "ms_per_step": ms_e2e / args.steps}
+        s.close()
+
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    sp, fp = results["split"], results["fp64"]
+    value = world * cells * args.steps / (sp["ms"] * 1e-3)
+    value64 = world * cells * args.steps / (fp["ms"] * 1e-3)
+    nj = sp["iters"] / args.steps
+    pk, src = peaks()
+    peak = float(pk["hbm_gbs"])
+    # dominant kernel class of the split step (eager profile of one step)
+    pr = sp["prof"]
+    classes = {"rhs": (pr["rhs_ms"], pr["rhs_launches"]),
+               "patankar_assemble": (pr["assemble_ms"], pr["assemble_launches"]),
+               "jacobi": (pr["jacobi_ms"], pr["jacobi_launches"])}
+    dom = max(classes, key=lambda k: classes[k][0])
+    prof_iters = sum(results["split"]["prof"].get("iters", []) or []) or nj
+    # algorithmic bytes per launch (per-cell figures of the byte model)
+    if dom == "jacobi":
+        alg = 64.0 * cells * prof_iters / max(classes[dom][1], 1)
+    elif dom == "rhs":
+        alg = 40.0 * cells
+    else:
+        alg = 80.0 * cells
+    t_launch = classes[dom][0] / max(classes[dom][1], 1) * 1e-3
+    achieved = alg / t_launch / 1e9
+    launches = sum(v[1] for v in classes.values()) + 1  # + dt reduction
+    line = {
+        "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": sp["ms"] / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64", "data": "synthetic",
+        "config": {"workload": f"island {c['nx']}x{c['ny']} periodic (wave over dry island), "
+                               f"mPDeC5, CFL 0.4, split precision, stencil Jacobi block {args.block}",
+                   "cells": cells, "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                   "l2": "inputs larger than L2 (~1.5 GB of state and stage arrays per step)"},
+        "fp64": {"value": value64, "ms_per_step": fp["ms"] / args.steps,
+                 "jacobi_iters_per_step": fp["iters"] / args.steps},
+        "split_over_fp64": value / value64,
+        "accuracy": {"rel_l1_split_vs_fp64_per_var": l1, "min_h": hmin,
+                     "steps": args.steps + args.warmup},
+        "jacobi_iters_per_step": nj,
+        "kernel_ms_per_step": {k: v[0] for k, v in classes.items()},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                     "peak_source": src},
+        "gpu_launches": launches * args.steps,
+        "clocks": clocks,
+        "e2e": e2e,
+    }
+    if not args.no_cpu:
+        try:
+            line["cpu_baseline"] = cpu_sample()
+        except Exception as exc:  # the baseline must not hide the GPU number
+            line["cpu_baseline"] = {"value": None, "error": str(exc)}
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

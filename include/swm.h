@@ -1,0 +1,178 @@
+/*
+ * swm.h -- C ABI of the B200 (sm_100a) mPDeC5 shallow-water time step.
+ *
+ * This is the drop-in boundary for the reference's time step in
+ * accdavlo/sw-mpdec (Fortran 90).  The reference exposes the step as two
+ * module procedures that share all state through module globals:
+ *   REAL FUNCTION TimeStep()                        equation.f90:791-837
+ *   SUBROUTINE TimeDiscretizationByMPDeC5(t)        timediscretization.f90:458-566
+ *   SUBROUTINE TimeDiscretizationByMPDeC2(t)        timediscretization.f90:571-664
+ * called from the driver loop at timediscretization.f90:58,71-72,75-76.
+ * The Fortran driver keeps t, dt, output cadence and I/O; it calls these
+ * entry points through ISO_C_BINDING (sw-mpdec_b200/fortran/mod_swm_capi.f90).
+ *
+ * Conventions
+ *  - Every call returns an int status: 0 ok, >0 warning, <0 error.
+ *  - Host arrays are owned by the caller and are copied in/out; the library
+ *    never retains a host pointer.  The library owns all device memory, its
+ *    stream and its CUDA graphs.  State stays on the device between steps.
+ *  - Ghosted state arrays use the reference's layout U(1:3,-2:nx+3,-2:ny+3):
+ *    column-major, variable fastest, 3*(nx+6)*(ny+6) doubles
+ *    (finitevolume.f90:139).  Only the interior is read on input.
+ *  - One handle per host thread; calls on a handle are synchronous unless
+ *    documented otherwise.
+ */
+#ifndef SWM_H
+#define SWM_H
+
+#if defined(__GNUC__)
+#define SWM_API __attribute__((visibility("default")))
+#else
+#define SWM_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define SWM_OK 0
+#define SWM_WARN_JACOBI_MAXITER 1 /* jacobi_iteration.f90:83-85 prints and continues */
+#define SWM_ERR_PARAM (-1)        /* invalid parameters (parameters.f90:123-126 STOPs) */
+#define SWM_ERR_CUDA (-2)         /* CUDA runtime error */
+#define SWM_ERR_NAN (-3)          /* non-finite state detected */
+#define SWM_ERR_WATCHDOG (-4)     /* a bounded device wait gave up */
+#define SWM_ERR_ALLOC (-5)        /* device or host allocation failed */
+#define SWM_ERR_STATE (-6)        /* call out of order (e.g. no state set) */
+#define SWM_ERR_UNSUPPORTED (-7)  /* option not available on this device */
+
+/* ---- option enums ---- */
+/* The reference's WENO weights use eps = 1e-24 on absolute values, so where a
+ * stencil varies by less than ~1e-7 its smoothness indicators are rounding noise
+ * and any change of arithmetic (FMA contraction, reciprocals) moves face values by
+ * up to that variation.  Parity at relative L1 1e-12 therefore needs the
+ * reference's own expression order: that is the plain FP64 form. */
+#define SWM_PREC_FP64 0     /* FP64 in the reference's expression order, no contraction */
+#define SWM_PREC_SPLIT 1    /* FP32 WENO on deviations from the cell value, FP64 rest */
+#define SWM_PREC_FP64_FMA 2 /* FP64 with FMA contraction and shared reciprocals */
+
+#define SWM_SOLVER_CSR 0     /* Jacobi on the reference CSR layout (finitevolume.f90:219-271) */
+#define SWM_SOLVER_STENCIL 1 /* matrix-free 5-point Jacobi, shared-memory temporal blocking */
+
+#define SWM_BATHY_FLAT 0
+#define SWM_BATHY_SINCOS 1 /* equation.f90:430 */
+#define SWM_BATHY_BUMP 2   /* equation.f90:433-438 */
+#define SWM_BATHY_GAUSS 3  /* A exp(-(ax (x-cx)^2 + ay (y-cy)^2)); par = {A, ax, cx, ay, cy} */
+
+typedef struct swm_params {
+  int nx, ny;            /* nElemsX, nElemsY (parameters.f90:66-120) */
+  double x0[2], x1[2];   /* MESH_X0, MESH_X1 */
+  double g;              /* Gravity */
+  double cfl;            /* CFL (parameters.f90:139) */
+  int timescheme;        /* 5 = mPDeC5, 7 = mPDeC2 (parameters.f90:144) */
+  int bathy_flag;        /* BathymetryFlag */
+  double bathy_par[5];   /* SWM_BATHY_GAUSS parameters */
+  int well_balanced;     /* -DWELLBALANCED (src/makefile:48) */
+  int precision;         /* SWM_PREC_* */
+  int solver;            /* SWM_SOLVER_* */
+  int jacobi_maxiter;    /* maxIter = 1000 (jacobi_iteration.f90:64) */
+  double jacobi_tol;     /* tolerance = 1e-16 (jacobi_iteration.f90:63) */
+  int jacobi_block;      /* stencil solver: Jacobi sweeps per pass (1..8), 0 = auto */
+  int mpdec2_compat;     /* 1: reproduce mPDeC2's hp(2,nx,ny) read of Up(:,1,:,:) */
+  int use_graph;         /* capture each step into a CUDA graph (1 = default) */
+  int device;            /* CUDA device ordinal */
+} swm_params;
+
+typedef struct swm_stats {
+  int status;                 /* status of the last step */
+  int n_solves;               /* Patankar solves in the last step (13 for mPDeC5) */
+  int jacobi_iters[16];       /* Jacobi iterations of each solve of the last step */
+  int jacobi_iters_min, jacobi_iters_max;
+  long long jacobi_iters_total; /* over all steps */
+  long long steps;            /* steps taken */
+  double lambda_max[2];       /* LambdaMaxX, LambdaMaxY of the last swm_timestep */
+} swm_stats;
+
+typedef struct swm_solver *swm_handle;
+
+/* Fill *p with the reference defaults (CFL 1.0, mPDeC5, tol 1e-16, maxIter 1000,
+ * FP64, CSR solver, graphs on) for an nx*ny grid on [x0,x1]. */
+SWM_API int swm_params_default(swm_params *p, int nx, int ny, double x00, double x01, double x10,
+                       double x11);
+
+/* Allocate device state for one grid (replaces InitializeFiniteVolume's
+ * allocation and CSR pattern build, finitevolume.f90:129-271). */
+SWM_API int swm_create(const swm_params *p, swm_handle *out);
+SWM_API int swm_destroy(swm_handle h);
+
+/* Copy the state U (ghosted layout) to the device. */
+SWM_API int swm_set_state(swm_handle h, const double *U_ghosted);
+/* Copy the device state back; V_ghosted (nullable) receives ConsToPrim of the
+ * state with periodic ghosts, as BoundaryConditions leaves V (equation.f90:778-782). */
+SWM_API int swm_get_state(swm_handle h, double *U_ghosted, double *V_ghosted);
+/* Interior state as three planes [3][ny][nx] (x fastest); host arrays. */
+SWM_API int swm_set_planes(swm_handle h, const double *planes);
+SWM_API int swm_get_planes(swm_handle h, double *planes);
+
+/* Well-balanced reference state (InitializeWBVariables, finitevolume.f90:339-396):
+ * runs one RHS on Uwb with the live kernel and precision and keeps FXWB, FYWB, SWB. */
+SWM_API int swm_set_wb_state(swm_handle h, const double *Uwb_ghosted);
+
+/* TimeStep() (equation.f90:791-837): CFL time step of the current state. */
+SWM_API int swm_timestep(swm_handle h, double *dt_min);
+
+/* One mPDeC5 (or mPDeC2) step of size dt from time t; the state is updated on
+ * the device.  Replaces TimeDiscretizationByMPDeC5(t) (timediscretization.f90:458-566).
+ * Returns SWM_WARN_JACOBI_MAXITER if a solve stopped at maxIter. */
+SWM_API int swm_step(swm_handle h, double t, double dt);
+
+/* Steps from t to t_end with dt = min(TimeStep(), t_out - t, t_end - t), restating
+ * the driver loop of timediscretization.f90:57-95 (output times every
+ * t_end/n_outputs) without I/O; returns the number of steps in *n_steps. */
+SWM_API int swm_run(swm_handle h, double t_end, int n_outputs, int *n_steps, double *t_reached);
+
+SWM_API int swm_get_stats(swm_handle h, swm_stats *s);
+/* Device-side totals of the state: mass sum(h), min(h), for invariant checks. */
+SWM_API int swm_state_summary(swm_handle h, double *mass, double *min_h);
+
+/* The cudaStream_t the handle launches on (for CUDA-event timing by the caller). */
+SWM_API int swm_get_stream(swm_handle h, void **stream);
+/* One step like swm_step, launched eagerly with CUDA events around every kernel:
+ * ms[0..3] = device milliseconds spent in the RHS, assembly and Jacobi kernels and
+ * the whole step; launches[0..2] = launches of each of the three classes. */
+SWM_API int swm_profile_step(swm_handle h, double t, double dt, float *ms, int *launches);
+
+/* Message for the last error on this thread (static storage). */
+SWM_API const char *swm_last_error(void);
+SWM_API const char *swm_strerror(int status);
+
+/* ---- diagnostics (parity tests) ---- */
+/* One RHS (FVTimeDerivative, finitevolume.f90:402-540) of the ghosted input
+ * state.  Outputs (nullable, column-major like the reference):
+ * Ut(3,nx,ny) [only Ut(2:3) computed, Ut(1)=0 as in the PATANKAR build],
+ * FX(3,0:nx,1:ny), FY(3,1:nx,0:ny), S(3,nx,ny): WB-subtracted when WB is on. */
+SWM_API int swm_debug_rhs(swm_handle h, const double *U_ghosted, double *Ut, double *FX, double *FY,
+                  double *S);
+/* Jacobi (jacobi_iteration.f90:52-87) on a user system given in the reference's
+ * CSR values: mass[5N] (slot order S,W,C,E,N), diag[N], rhs[N] -> sol[N];
+ * runs the handle's solver (CSR or stencil) and returns the iteration count. */
+SWM_API int swm_debug_jacobi(swm_handle h, const double *mass, const double *diag, const double *rhs,
+                     double *sol, int *iters);
+
+/* ---- batched ensembles ---- */
+typedef struct swm_batch *swm_batch_handle;
+/* n problems of independent size and parameters, stepped together: one
+ * persistent launch per phase covers every problem's tiles. */
+SWM_API int swm_batch_create(int n, const swm_params *p, swm_batch_handle *out);
+SWM_API int swm_batch_destroy(swm_batch_handle b);
+SWM_API int swm_batch_set_planes(swm_batch_handle b, int i, const double *planes);
+SWM_API int swm_batch_get_planes(swm_batch_handle b, int i, double *planes);
+/* One step of every problem, each with its own dt = TimeStep() (computed on
+ * the device); dt_out[n] (nullable) receives the steps taken. */
+SWM_API int swm_batch_step(swm_batch_handle b, double *dt_out);
+SWM_API int swm_batch_cells(swm_batch_handle b, long long *cells);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SWM_H */

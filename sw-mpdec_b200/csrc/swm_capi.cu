@@ -1,0 +1,953 @@
+// swm_capi.cu -- C ABI (include/swm.h) and host orchestration of one mPDeC step.
+//
+// Replaces the reference's module procedures TimeStep() (equation.f90:791-837)
+// and TimeDiscretizationByMPDeC5/2(t) (timediscretization.f90:458-664).  The
+// state lives on the device as three planes [ny][nx]; one step is the fixed
+// sequence of kernels below, captured once into a CUDA graph (dt is read from
+// device memory, so the graph is replayed unchanged every step).
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/swm.h"
+#include "swm_kernels.cuh"
+
+using namespace swm;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+#define CK(call)                                                                         \
+  do {                                                                                   \
+    cudaError_t e_ = (call);                                                             \
+    if (e_ != cudaSuccess)                                                               \
+      return fail(SWM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));     \
+  } while (0)
+
+// thetaDeC (timediscretization.f90:491-506), row m, column r, row-major [m][r]
+const double kTheta5[4][4] = {
+    {0.0000000000000000000, 0.0000000000000000000, 0.0000000000000000000, 0.0000000000000000000},
+    {0.1103005664791649049, 0.1896994335208351257, -0.0339073642291439076, 0.0103005664791649201},
+    {0.0730327668541684294, 0.4505740308958107176, 0.2269672331458314485, -0.0269672331458315692},
+    {0.0833333333333333287, 0.4166666666666666852, 0.4166666666666666852, 0.0833333333333333287}};
+// mPDeC2 (timediscretization.f90:604)
+const double kTheta2[2][2] = {{0.0, 0.0}, {0.5, 0.5}};
+
+}  // namespace
+
+struct swm_solver {
+  swm_params p{};
+  int nx = 0, ny = 0;
+  size_t N = 0;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  Grid gr{};
+  std::vector<void*> allocs;
+  // state U^n
+  double *h = nullptr, *hu = nullptr, *hv = nullptr;
+  // substep states Ua(m) for m = 2..4 (index m-1); depth double-buffered by correction parity
+  double* hbuf[4][2] = {};
+  double* hum[4] = {};
+  double* hvm[4] = {};
+  // stage RHS slots r = 1..4 (index r-1)
+  double* fu[4] = {};
+  double* fv[4] = {};
+  double* fxm[4] = {};
+  double* fym[4] = {};
+  // Patankar system
+  double *cS = nullptr, *cW = nullptr, *cE = nullptr, *cN = nullptr, *cD = nullptr;
+  double *csr_mass = nullptr, *csr_diag = nullptr;
+  int *rowstart = nullptr, *cols = nullptr;
+  double *xa = nullptr, *xb = nullptr, *rhs_compat = nullptr;
+  // well-balanced reference
+  double *fxwb = nullptr, *fywb = nullptr, *swb = nullptr;
+  bool have_wb = false;
+  // bathymetry factor tables (Gaussian)
+  double *gex = nullptr, *gey = nullptr;
+  double* bgrad = nullptr;  // [4][4][2][N] b_x, b_y at interior Gauss points
+  // scalars
+  double* dt_dev = nullptr;
+  unsigned long long* lam = nullptr;
+  int* bad = nullptr;
+  JacobiCtl* ctl = nullptr;
+  double* summary = nullptr;
+  double* stage = nullptr;  // ghosted staging (3*(nx+6)*(ny+6))
+  double* stage2 = nullptr;
+  // pinned host mirrors
+  double* h_dt = nullptr;
+  JacobiCtl* h_ctl = nullptr;
+  unsigned long long* h_lam = nullptr;
+  int* h_bad = nullptr;
+  // graph
+  cudaGraphExec_t graph = nullptr;
+  bool graph_failed = false;
+  int jac_blocks = 0;
+  int n_solves = 0;
+  // per-launch event profiling (swm_profile_step)
+  bool profiling = false;
+  std::vector<cudaEvent_t> prof_ev;
+  std::vector<int> prof_cls;
+  // stats
+  swm_stats stats{};
+  bool have_state = false;
+
+  template <typename T>
+  int dalloc(T** ptr, size_t count) {
+    void* p_ = nullptr;
+    cudaError_t e = cudaMalloc(&p_, count * sizeof(T) + 64);
+    if (e != cudaSuccess) return fail(SWM_ERR_ALLOC, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    cudaMemset(p_, 0, count * sizeof(T) + 64);
+    allocs.push_back(p_);
+    *ptr = static_cast<T*>(p_);
+    return SWM_OK;
+  }
+};
+
+static int valid_params(const swm_params* p) {
+  if (!p) return fail(SWM_ERR_PARAM, "null params");
+  if (p->nx < 3 || p->ny < 3) return fail(SWM_ERR_PARAM, "nx, ny must be >= 3");
+  if ((long long)p->nx * p->ny > (1LL << 28)) return fail(SWM_ERR_PARAM, "grid too large");
+  if (p->timescheme != 5 && p->timescheme != 7)
+    return fail(SWM_ERR_PARAM, "timescheme must be 5 (mPDeC5) or 7 (mPDeC2)");
+  if (p->precision < 0 || p->precision > 2) return fail(SWM_ERR_PARAM, "unknown precision");
+  if (p->solver != SWM_SOLVER_CSR && p->solver != SWM_SOLVER_STENCIL)
+    return fail(SWM_ERR_PARAM, "unknown solver");
+  if (p->bathy_flag < 0 || p->bathy_flag > 3) return fail(SWM_ERR_PARAM, "unknown bathymetry");
+  if (p->jacobi_maxiter < 1) return fail(SWM_ERR_PARAM, "jacobi_maxiter must be >= 1");
+  if (!(p->jacobi_tol >= 0.0)) return fail(SWM_ERR_PARAM, "jacobi_tol must be >= 0");
+  if (p->jacobi_block < 0 || p->jacobi_block > kMaxBlock)
+    return fail(SWM_ERR_PARAM, "jacobi_block must be in 0..8");
+  if (!(p->x1[0] != p->x0[0]) || !(p->x1[1] != p->x0[1]))
+    return fail(SWM_ERR_PARAM, "empty domain");
+  if (!(p->g > 0.0) || !(p->cfl > 0.0)) return fail(SWM_ERR_PARAM, "g and cfl must be > 0");
+  return SWM_OK;
+}
+
+static void quadrature(double qn[4], double qw[4]) {
+  // mesh.f90:127-129
+  qw[0] = (18. - sqrt(30.)) / 72.;
+  qw[1] = (18. + sqrt(30.)) / 72.;
+  qw[2] = (18. + sqrt(30.)) / 72.;
+  qw[3] = (18. - sqrt(30.)) / 72.;
+  qn[0] = -(0.5 * sqrt(3. / 7. + 2. / 7. * sqrt(6. / 5.)));
+  qn[1] = -(0.5 * sqrt(3. / 7. - 2. / 7. * sqrt(6. / 5.)));
+  qn[2] = 0.5 * sqrt(3. / 7. - 2. / 7. * sqrt(6. / 5.));
+  qn[3] = 0.5 * sqrt(3. / 7. + 2. / 7. * sqrt(6. / 5.));
+}
+
+static double host_gp(double x0, double h, int c, double q) {
+  double node = x0 + ((double)c) * h;
+  double bary = node + 0.5 * h;
+  return bary + q * h;
+}
+
+// Bathymetry_X / Bathymetry_Y (equation.f90:451-509) and the Gaussian case, evaluated
+// on the host (this translation unit is built without FP contraction).
+static void host_bathy_grad(const swm_params& p, double x, double y, double* bx, double* by) {
+  const double PI = acos(-1.0);
+  *bx = 0.;
+  *by = 0.;
+  if (p.bathy_flag == SWM_BATHY_SINCOS) {
+    *bx = 0.1 * 2. * PI * cos(2. * PI * x) * cos(2. * PI * y);
+    *by = -(0.1 * 2. * PI * sin(2. * PI * x) * sin(2. * PI * y));
+  } else if (p.bathy_flag == SWM_BATHY_BUMP) {
+    double r2 = x * x + y * y;
+    if (r2 < 1) {
+      double d = 1.0 - r2;
+      double e = exp(1.0 - 1.0 / d);
+      *bx = -(2.0 * x / (d * d) * e);
+      *by = -(2.0 * y / (d * d) * e);
+    }
+  } else if (p.bathy_flag == SWM_BATHY_GAUSS) {
+    const double A = p.bathy_par[0], ax = p.bathy_par[1], cx = p.bathy_par[2];
+    const double ay = p.bathy_par[3], cy = p.bathy_par[4];
+    double dxv = x - cx, dyv = y - cy;
+    double e = exp(-(ax * (dxv * dxv) + ay * (dyv * dyv)));
+    double B = A * e;
+    *bx = (-2.0 * ax * dxv) * B;
+    *by = (-2.0 * ay * dyv) * B;
+  }
+}
+
+static int jacobi_block_of(const swm_params& p) {
+  if (p.solver == SWM_SOLVER_CSR) return 1;
+  return p.jacobi_block > 0 ? p.jacobi_block : 4;
+}
+
+static RhsArgs make_rhs_args(swm_solver* s, const double* h, const double* hu, const double* hv,
+                             int slot) {
+  RhsArgs a{};
+  a.gr = s->gr;
+  a.h = h;
+  a.hu = hu;
+  a.hv = hv;
+  a.ut_hu = s->fu[slot];
+  a.ut_hv = s->fv[slot];
+  a.fxm = s->fxm[slot];
+  a.fym = s->fym[slot];
+  if (s->have_wb && s->p.well_balanced) {
+    a.fx_wb = s->fxwb;
+    a.fy_wb = s->fywb;
+    a.s_wb = s->swb;
+  }
+  a.gauss_ex = s->gex;
+  a.gauss_ey = s->gey;
+  a.bgrad = s->bgrad;
+  return a;
+}
+
+static cudaError_t launch_rhs(swm_solver* s, const RhsArgs& a) {
+  if (s->p.precision == SWM_PREC_FP64) return launch_rhs_exact(a, s->stream);
+  return launch_rhs_fast(s->p.precision == SWM_PREC_SPLIT ? 1 : 0, a, s->stream);
+}
+
+static void fill_thresh(const swm_solver* s, unsigned long long t[3]) {
+  // stop when sum|dx| <= tol * n  (jacobi_iteration.f90:71,77)
+  residual_limbs_host(s->p.jacobi_tol * (double)s->N, t);
+}
+
+// Event pair around one launch when profiling (class 0 RHS, 1 assembly, 2 Jacobi).
+static void prof_mark(swm_solver* s, int cls) {
+  if (!s->profiling) return;
+  cudaEvent_t e;
+  cudaEventCreate(&e);
+  cudaEventRecord(e, s->stream);
+  s->prof_ev.push_back(e);
+  s->prof_cls.push_back(cls);
+}
+
+// Enqueue one complete mPDeC step on s->stream (dt read from s->dt_dev).
+static int enqueue_step(swm_solver* s) {
+  const bool two = (s->p.timescheme == 7);
+  const int ms = two ? 2 : 4, kc = two ? 2 : 5;
+  const bool csr = (s->p.solver == SWM_SOLVER_CSR);
+  const bool compat = two && s->p.mpdec2_compat;
+  CK(cudaMemsetAsync(&s->ctl->iters[0], 0, sizeof(int) * (kMaxSolves + 1), s->stream));
+  // RHS at U^n (timediscretization.f90:519), stored in slot 1 and used for all r at k=1
+  prof_mark(s, 0);
+  CK(launch_rhs(s, make_rhs_args(s, s->h, s->hu, s->hv, 0)));
+  prof_mark(s, -1);
+  int solve = 0;
+  for (int k = 1; k <= kc; ++k) {
+    const int mlo = (k == kc) ? ms : 2;
+    for (int m = mlo; m <= ms; ++m) {
+      AssembleArgs aa{};
+      aa.nx = s->nx;
+      aa.ny = s->ny;
+      aa.dx = s->gr.dx;
+      aa.dy = s->gr.dy;
+      aa.m = m;
+      aa.msteps = ms;
+      aa.compat2 = compat ? 1 : 0;
+      for (int r = 0; r < 4; ++r) aa.theta[r] = two ? (r < 2 ? kTheta2[m - 1][r] : 0.0) : kTheta5[m - 1][r];
+      aa.dt = s->dt_dev;
+      aa.hu_n = s->hu;
+      aa.hv_n = s->hv;
+      for (int r = 0; r < ms; ++r) {
+        const int slot = (k == 1) ? 0 : r;
+        aa.fu[r] = s->fu[slot];
+        aa.fv[r] = s->fv[slot];
+        aa.fxm[r] = s->fxm[slot];
+        aa.fym[r] = s->fym[slot];
+        aa.hp[r] = (r == 0 || k == 1) ? s->h : s->hbuf[r][(k - 1) & 1];
+      }
+      const bool last = (k == kc);
+      aa.hu_out = last ? s->hu : s->hum[m - 1];
+      aa.hv_out = last ? s->hv : s->hvm[m - 1];
+      aa.cS = s->cS;
+      aa.cW = s->cW;
+      aa.cE = s->cE;
+      aa.cN = s->cN;
+      aa.cD = s->cD;
+      aa.csr_mass = s->csr_mass;
+      aa.csr_diag = s->csr_diag;
+      aa.rhs_out = compat ? s->rhs_compat : nullptr;
+      prof_mark(s, 1);
+      CK(launch_assemble(aa, csr, s->stream));
+      prof_mark(s, -1);
+      JacobiArgs ja{};
+      ja.nx = s->nx;
+      ja.ny = s->ny;
+      ja.solve_idx = solve < kMaxSolves ? solve : kMaxSolves - 1;
+      ja.maxiter = s->p.jacobi_maxiter;
+      fill_thresh(s, ja.thresh);
+      ja.b = compat ? s->rhs_compat : s->h;
+      ja.cS = s->cS;
+      ja.cW = s->cW;
+      ja.cE = s->cE;
+      ja.cN = s->cN;
+      ja.cD = s->cD;
+      ja.rowstart = s->rowstart;
+      ja.cols = s->cols;
+      ja.mass = s->csr_mass;
+      ja.diag = s->csr_diag;
+      ja.xa = s->xa;
+      ja.xb = s->xb;
+      ja.out = last ? s->h : s->hbuf[m - 1][k & 1];
+      ja.ctl = s->ctl;
+      ja.block = jacobi_block_of(s->p);
+      ja.spin_limit = 1LL << 26;
+      prof_mark(s, 2);
+      CK(launch_jacobi(ja, csr, s->jac_blocks, s->stream));
+      prof_mark(s, -1);
+      solve++;
+    }
+    if (k < kc) {  // RHS at Ua(m) (timediscretization.f90:550-557)
+      for (int m = 2; m <= ms; ++m) {
+        prof_mark(s, 0);
+        CK(launch_rhs(s, make_rhs_args(s, s->hbuf[m - 1][k & 1], s->hum[m - 1], s->hvm[m - 1],
+                                       m - 1)));
+        prof_mark(s, -1);
+      }
+    }
+  }
+  s->n_solves = solve;
+  return SWM_OK;
+}
+
+static int build_graph(swm_solver* s) {
+  if (s->graph || s->graph_failed || !s->p.use_graph) return SWM_OK;
+  cudaGraph_t g = nullptr;
+  if (cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    cudaGetLastError();
+    s->graph_failed = true;
+    return SWM_OK;
+  }
+  int rc = enqueue_step(s);
+  cudaError_t e = cudaStreamEndCapture(s->stream, &g);
+  if (rc != SWM_OK || e != cudaSuccess || !g) {
+    cudaGetLastError();
+    if (g) cudaGraphDestroy(g);
+    s->graph_failed = true;
+    return SWM_OK;
+  }
+  e = cudaGraphInstantiate(&s->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    s->graph = nullptr;
+    s->graph_failed = true;
+  }
+  return SWM_OK;
+}
+
+static void drop_graph(swm_solver* s) {
+  if (s->graph) cudaGraphExecDestroy(s->graph);
+  s->graph = nullptr;
+  s->graph_failed = false;
+}
+
+extern "C" {
+
+int swm_params_default(swm_params* p, int nx, int ny, double x00, double x01, double x10,
+                       double x11) {
+  if (!p) return fail(SWM_ERR_PARAM, "null params");
+  std::memset(p, 0, sizeof(*p));
+  p->nx = nx;
+  p->ny = ny;
+  p->x0[0] = x00;
+  p->x0[1] = x01;
+  p->x1[0] = x10;
+  p->x1[1] = x11;
+  p->g = 9.81;
+  p->cfl = 1.0;
+  p->timescheme = 5;
+  p->bathy_flag = 0;
+  p->well_balanced = 0;
+  p->precision = SWM_PREC_FP64;
+  p->solver = SWM_SOLVER_CSR;
+  p->jacobi_maxiter = 1000;
+  p->jacobi_tol = 1.0e-16;
+  p->jacobi_block = 0;
+  p->mpdec2_compat = 0;
+  p->use_graph = 1;
+  p->device = 0;
+  return SWM_OK;
+}
+
+int swm_create(const swm_params* p, swm_handle* out) {
+  if (!out) return fail(SWM_ERR_PARAM, "null handle pointer");
+  *out = nullptr;
+  int rc = valid_params(p);
+  if (rc) return rc;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return fail(SWM_ERR_CUDA, "no CUDA device available");
+  if (p->device < 0 || p->device >= ndev) return fail(SWM_ERR_PARAM, "invalid device ordinal");
+  CK(cudaSetDevice(p->device));
+  int major = 0, minor = 0;
+  cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, p->device);
+  cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, p->device);
+  if (major != 10 || minor != 0)
+    return fail(SWM_ERR_UNSUPPORTED, "this build targets sm_100a (B200) only");
+  int coop = 0;
+  cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, p->device);
+  if (!coop) return fail(SWM_ERR_UNSUPPORTED, "cooperative launch not supported");
+
+  swm_solver* s = new swm_solver();
+  s->p = *p;
+  s->device = p->device;
+  s->nx = p->nx;
+  s->ny = p->ny;
+  s->N = (size_t)p->nx * p->ny;
+  // mesh.f90:58-60 and quadrature
+  Grid& gr = s->gr;
+  gr.nx = s->nx;
+  gr.ny = s->ny;
+  gr.x0 = p->x0[0];
+  gr.y0 = p->x0[1];
+  gr.dx = fabs(fabs(p->x1[0] - p->x0[0])) / ((double)s->nx);
+  gr.dy = fabs(fabs(p->x1[1] - p->x0[1])) / ((double)s->ny);
+  gr.g = p->g;
+  gr.bathy = p->bathy_flag;
+  for (int k = 0; k < 5; ++k) gr.bp[k] = p->bathy_par[k];
+  quadrature(gr.qn, gr.qw);
+  for (int a = 0; a < 4; ++a)
+    for (int b = 0; b < 4; ++b) gr.wgp[a][b] = gr.qw[a] * gr.qw[b];
+
+  auto cleanup = [&](int code) {
+    swm_destroy(s);
+    return code;
+  };
+  if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return cleanup(fail(SWM_ERR_CUDA, "cudaStreamCreate failed"));
+  const size_t N = s->N, nx = s->nx, ny = s->ny;
+  const size_t nfx = (nx + 1) * ny, nfy = nx * (ny + 1);
+  const bool csr = p->solver == SWM_SOLVER_CSR;
+#define AL(ptr, cnt)                          \
+  do {                                        \
+    int rc_ = s->dalloc(&(ptr), (cnt));       \
+    if (rc_) return cleanup(rc_);             \
+  } while (0)
+  AL(s->h, N);
+  AL(s->hu, N);
+  AL(s->hv, N);
+  for (int m = 1; m < 4; ++m) {
+    AL(s->hbuf[m][0], N);
+    AL(s->hbuf[m][1], N);
+    AL(s->hum[m], N);
+    AL(s->hvm[m], N);
+  }
+  for (int r = 0; r < 4; ++r) {
+    AL(s->fu[r], N);
+    AL(s->fv[r], N);
+    AL(s->fxm[r], nfx);
+    AL(s->fym[r], nfy);
+  }
+  if (csr) {
+    AL(s->csr_mass, 5 * N);
+    AL(s->csr_diag, N);
+    AL(s->rowstart, N + 1);
+    AL(s->cols, 5 * N);
+  } else {
+    AL(s->cS, N);
+    AL(s->cW, N);
+    AL(s->cE, N);
+    AL(s->cN, N);
+    AL(s->cD, N);
+  }
+  AL(s->xa, N);
+  AL(s->xb, N);
+  if (p->timescheme == 7 && p->mpdec2_compat) AL(s->rhs_compat, N);
+  if (p->well_balanced) {
+    AL(s->fxwb, 3 * nfx);
+    AL(s->fywb, 3 * nfy);
+    AL(s->swb, 3 * N);
+  }
+  AL(s->dt_dev, 1);
+  AL(s->lam, 2);
+  AL(s->bad, 1);
+  AL(s->ctl, 1);
+  AL(s->summary, 2 + 512);
+  AL(s->stage, 3 * (nx + 6) * (ny + 6));
+  AL(s->stage2, 3 * (nx + 6) * (ny + 6));
+#undef AL
+  if (cudaMallocHost(&s->h_dt, sizeof(double)) != cudaSuccess ||
+      cudaMallocHost(&s->h_ctl, sizeof(JacobiCtl)) != cudaSuccess ||
+      cudaMallocHost(&s->h_lam, 2 * sizeof(unsigned long long)) != cudaSuccess ||
+      cudaMallocHost(&s->h_bad, sizeof(int)) != cudaSuccess)
+    return cleanup(fail(SWM_ERR_ALLOC, "cudaMallocHost failed"));
+
+  if (csr) {  // finitevolume.f90:219-267 CSR pattern, 1-based, slot order S, W, C, E, N
+    std::vector<int> rs(N + 1), cl(5 * N);
+    auto ge = [&](int ii, int jj) {  // mesh.f90:168 GlobalElem
+      int a = (jj - 1) % (int)ny;
+      if (a < 0) a += ny;
+      int b = (ii - 1) % (int)nx;
+      if (b < 0) b += nx;
+      return a * (int)nx + b + 1;
+    };
+    int isv = 0, irs = 0;
+    for (int jj = 1; jj <= (int)ny; ++jj)
+      for (int ii = 1; ii <= (int)nx; ++ii) {
+        isv++;
+        irs++;
+        rs[irs - 1] = isv;
+        cl[isv - 1] = ge(ii, jj - 1);
+        isv++;
+        cl[isv - 1] = ge(ii - 1, jj);
+        isv++;
+        cl[isv - 1] = ge(ii, jj);
+        isv++;
+        cl[isv - 1] = ge(ii + 1, jj);
+        isv++;
+        cl[isv - 1] = ge(ii, jj + 1);
+      }
+    rs[N] = rs[N - 1] + 5;
+    if (cudaMemcpy(s->rowstart, rs.data(), sizeof(int) * (N + 1), cudaMemcpyHostToDevice) !=
+            cudaSuccess ||
+        cudaMemcpy(s->cols, cl.data(), sizeof(int) * 5 * N, cudaMemcpyHostToDevice) != cudaSuccess)
+      return cleanup(fail(SWM_ERR_CUDA, "CSR upload failed"));
+  }
+  if (p->bathy_flag == SWM_BATHY_GAUSS && p->precision != SWM_PREC_FP64) {
+    // separable Gaussian factors at the Gauss nodes (split and FMA forms)
+    int rc2 = s->dalloc(&s->gex, 4 * nx);
+    if (!rc2) rc2 = s->dalloc(&s->gey, 4 * ny);
+    if (rc2) return cleanup(rc2);
+    std::vector<double> ex(4 * nx), ey(4 * ny);
+    for (size_t i = 0; i < nx; ++i)
+      for (int q = 0; q < 4; ++q) {
+        double d = host_gp(gr.x0, gr.dx, (int)i, gr.qn[q]) - gr.bp[2];
+        ex[4 * i + q] = exp(-(gr.bp[1] * (d * d)));
+      }
+    for (size_t j = 0; j < ny; ++j)
+      for (int q = 0; q < 4; ++q) {
+        double d = host_gp(gr.y0, gr.dy, (int)j, gr.qn[q]) - gr.bp[4];
+        ey[4 * j + q] = exp(-(gr.bp[3] * (d * d)));
+      }
+    cudaMemcpy(s->gex, ex.data(), sizeof(double) * 4 * nx, cudaMemcpyHostToDevice);
+    cudaMemcpy(s->gey, ey.data(), sizeof(double) * 4 * ny, cudaMemcpyHostToDevice);
+  }
+  const bool full_table =
+      p->bathy_flag > 0 && (p->precision == SWM_PREC_FP64 || p->bathy_flag != SWM_BATHY_GAUSS);
+  if (full_table) {  // b_x, b_y at the 16 interior Gauss points, host libm (equation.f90:451-509)
+    int rc2 = s->dalloc(&s->bgrad, 32 * N);
+    if (rc2) return cleanup(rc2);
+    std::vector<double> tab(32 * N);
+    std::vector<double> X(4 * nx), Y(4 * ny);
+    for (size_t i = 0; i < nx; ++i)
+      for (int q = 0; q < 4; ++q) X[4 * i + q] = host_gp(gr.x0, gr.dx, (int)i, gr.qn[q]);
+    for (size_t j = 0; j < ny; ++j)
+      for (int q = 0; q < 4; ++q) Y[4 * j + q] = host_gp(gr.y0, gr.dy, (int)j, gr.qn[q]);
+    for (int a = 0; a < 4; ++a)
+      for (int b = 0; b < 4; ++b)
+        for (size_t j = 0; j < ny; ++j)
+          for (size_t i = 0; i < nx; ++i) {
+            double bx, by;
+            host_bathy_grad(*p, X[4 * i + a], Y[4 * j + b], &bx, &by);
+            tab[((a * 4 + b) * 2 + 0) * N + j * nx + i] = bx;
+            tab[((a * 4 + b) * 2 + 1) * N + j * nx + i] = by;
+          }
+    if (cudaMemcpy(s->bgrad, tab.data(), sizeof(double) * 32 * N, cudaMemcpyHostToDevice) !=
+        cudaSuccess)
+      return cleanup(fail(SWM_ERR_CUDA, "bathymetry table upload failed"));
+  }
+  s->jac_blocks = jacobi_grid_blocks(csr, jacobi_block_of(s->p), s->device);
+  if (s->jac_blocks < 1) return cleanup(fail(SWM_ERR_CUDA, "Jacobi kernel cannot be resident"));
+  // the RHS kernels' shared-memory attribute is set on first launch
+  if (cudaDeviceSynchronize() != cudaSuccess)
+    return cleanup(fail(SWM_ERR_CUDA, "initialisation failed"));
+  s->stats.jacobi_iters_min = 0;
+  *out = s;
+  return SWM_OK;
+}
+
+int swm_destroy(swm_handle s) {
+  if (!s) return SWM_OK;
+  cudaSetDevice(s->device);
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  drop_graph(s);
+  for (void* ptr : s->allocs) cudaFree(ptr);
+  if (s->h_dt) cudaFreeHost(s->h_dt);
+  if (s->h_ctl) cudaFreeHost(s->h_ctl);
+  if (s->h_lam) cudaFreeHost(s->h_lam);
+  if (s->h_bad) cudaFreeHost(s->h_bad);
+  if (s->stream) cudaStreamDestroy(s->stream);
+  delete s;
+  return SWM_OK;
+}
+
+static int upload_ghosted(swm_solver* s, const double* U, double* h, double* hu, double* hv) {
+  const size_t cnt = 3 * (size_t)(s->nx + 6) * (s->ny + 6);
+  CK(cudaMemcpyAsync(s->stage, U, cnt * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+  CK(launch_ghosted_to_planes(s->stage, s->nx, s->ny, h, hu, hv, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return SWM_OK;
+}
+
+int swm_set_state(swm_handle s, const double* U) {
+  if (!s || !U) return fail(SWM_ERR_PARAM, "null argument");
+  CK(cudaSetDevice(s->device));
+  int rc = upload_ghosted(s, U, s->h, s->hu, s->hv);
+  if (rc) return rc;
+  s->have_state = true;
+  return SWM_OK;
+}
+
+int swm_get_state(swm_handle s, double* U, double* V) {
+  if (!s || !U) return fail(SWM_ERR_PARAM, "null argument");
+  if (!s->have_state) return fail(SWM_ERR_STATE, "no state set");
+  CK(cudaSetDevice(s->device));
+  const size_t cnt = 3 * (size_t)(s->nx + 6) * (s->ny + 6);
+  CK(launch_planes_to_ghosted(s->h, s->hu, s->hv, s->nx, s->ny, s->stage, V ? s->stage2 : nullptr,
+                              s->stream));
+  CK(cudaMemcpyAsync(U, s->stage, cnt * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  if (V) CK(cudaMemcpyAsync(V, s->stage2, cnt * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return SWM_OK;
+}
+
+int swm_set_planes(swm_handle s, const double* P) {
+  if (!s || !P) return fail(SWM_ERR_PARAM, "null argument");
+  CK(cudaSetDevice(s->device));
+  CK(cudaMemcpyAsync(s->h, P, s->N * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+  CK(cudaMemcpyAsync(s->hu, P + s->N, s->N * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+  CK(cudaMemcpyAsync(s->hv, P + 2 * s->N, s->N * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  s->have_state = true;
+  return SWM_OK;
+}
+
+int swm_get_planes(swm_handle s, double* P) {
+  if (!s || !P) return fail(SWM_ERR_PARAM, "null argument");
+  if (!s->have_state) return fail(SWM_ERR_STATE, "no state set");
+  CK(cudaSetDevice(s->device));
+  CK(cudaMemcpyAsync(P, s->h, s->N * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaMemcpyAsync(P + s->N, s->hu, s->N * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaMemcpyAsync(P + 2 * s->N, s->hv, s->N * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return SWM_OK;
+}
+
+int swm_set_wb_state(swm_handle s, const double* Uwb) {
+  if (!s || !Uwb) return fail(SWM_ERR_PARAM, "null argument");
+  if (!s->p.well_balanced) return fail(SWM_ERR_STATE, "handle created without well_balanced");
+  CK(cudaSetDevice(s->device));
+  // scratch planes: substep-2 buffers are free between steps
+  double *h = s->hbuf[1][0], *hu = s->hum[1], *hv = s->hvm[1];
+  int rc = upload_ghosted(s, Uwb, h, hu, hv);
+  if (rc) return rc;
+  RhsArgs a = make_rhs_args(s, h, hu, hv, 1);
+  a.fx_wb = a.fy_wb = a.s_wb = nullptr;  // FXWB = 0 during InitializeWBVariables
+  a.fx_full = s->fxwb;
+  a.fy_full = s->fywb;
+  a.s_full = s->swb;
+  CK(launch_rhs(s, a));
+  CK(cudaStreamSynchronize(s->stream));
+  s->have_wb = true;
+  drop_graph(s);  // the step graph bakes the WB pointers in
+  return SWM_OK;
+}
+
+int swm_timestep(swm_handle s, double* dt_min) {
+  if (!s || !dt_min) return fail(SWM_ERR_PARAM, "null argument");
+  if (!s->have_state) return fail(SWM_ERR_STATE, "no state set");
+  CK(cudaSetDevice(s->device));
+  CK(cudaMemsetAsync(s->lam, 0, 2 * sizeof(unsigned long long), s->stream));
+  CK(cudaMemsetAsync(s->bad, 0, sizeof(int), s->stream));
+  DtArgs a{s->nx, s->ny, s->p.g, s->h, s->hu, s->hv, s->lam, s->bad};
+  CK(launch_dt(a, s->stream));
+  CK(cudaMemcpyAsync(s->h_lam, s->lam, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                     s->stream));
+  CK(cudaMemcpyAsync(s->h_bad, s->bad, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  double LX, LY;
+  std::memcpy(&LX, &s->h_lam[0], sizeof(double));
+  std::memcpy(&LY, &s->h_lam[1], sizeof(double));
+  s->stats.lambda_max[0] = LX;
+  s->stats.lambda_max[1] = LY;
+  // equation.f90:818-834
+  double ts = 1.7976931348623157e308;  // HUGE(1.0)
+  double a1 = s->gr.dx / LX, b1 = s->gr.dy / LY;
+  if (a1 < ts) ts = a1;
+  if (b1 < ts) ts = b1;
+  ts = s->p.cfl * ts;
+  if (ts < 1.0e-30) ts = 1.0e-30;
+  *dt_min = ts;
+  if (*s->h_bad) return fail(SWM_ERR_NAN, "non-finite or negative depth in the state");
+  return SWM_OK;
+}
+
+int swm_step(swm_handle s, double t, double dt) {
+  (void)t;  // stage times are not read by the periodic BC or the source (equation.f90:515,284)
+  if (!s) return fail(SWM_ERR_PARAM, "null handle");
+  if (!s->have_state) return fail(SWM_ERR_STATE, "no state set");
+  if (!(dt > 0.0) || !std::isfinite(dt)) return fail(SWM_ERR_PARAM, "dt must be finite and > 0");
+  if (s->p.well_balanced && !s->have_wb)
+    return fail(SWM_ERR_STATE, "well_balanced handle without swm_set_wb_state");
+  CK(cudaSetDevice(s->device));
+  *s->h_dt = dt;
+  CK(cudaMemcpyAsync(s->dt_dev, s->h_dt, sizeof(double), cudaMemcpyHostToDevice, s->stream));
+  int rc = build_graph(s);
+  if (rc) return rc;
+  if (s->graph) {
+    CK(cudaGraphLaunch(s->graph, s->stream));
+  } else {
+    rc = enqueue_step(s);
+    if (rc) return rc;
+  }
+  CK(cudaMemcpyAsync(s->h_ctl, s->ctl, sizeof(JacobiCtl), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  if (s->n_solves == 0) {  // graph built without a host pass: count solves
+    s->n_solves = (s->p.timescheme == 7) ? 2 : 13;
+  }
+  const JacobiCtl& c = *s->h_ctl;
+  swm_stats& st = s->stats;
+  st.n_solves = s->n_solves;
+  st.jacobi_iters_min = 1 << 30;
+  st.jacobi_iters_max = 0;
+  for (int k = 0; k < s->n_solves && k < kMaxSolves; ++k) {
+    st.jacobi_iters[k] = c.iters[k];
+    st.jacobi_iters_total += c.iters[k];
+    if (c.iters[k] < st.jacobi_iters_min) st.jacobi_iters_min = c.iters[k];
+    if (c.iters[k] > st.jacobi_iters_max) st.jacobi_iters_max = c.iters[k];
+  }
+  st.steps++;
+  st.status = c.status;
+  if (c.status < 0) return fail(SWM_ERR_WATCHDOG, "Jacobi grid barrier watchdog expired");
+  if (c.status == 1) {
+    g_last_error = "Jacobi not converged (maxIter reached)";
+    return SWM_WARN_JACOBI_MAXITER;
+  }
+  return SWM_OK;
+}
+
+int swm_get_stream(swm_handle s, void** stream) {
+  if (!s || !stream) return fail(SWM_ERR_PARAM, "null argument");
+  *stream = (void*)s->stream;
+  return SWM_OK;
+}
+
+int swm_profile_step(swm_handle s, double t, double dt, float* ms, int* launches) {
+  if (!s || !ms) return fail(SWM_ERR_PARAM, "null argument");
+  if (!s->have_state) return fail(SWM_ERR_STATE, "no state set");
+  CK(cudaSetDevice(s->device));
+  *s->h_dt = dt;
+  CK(cudaMemcpyAsync(s->dt_dev, s->h_dt, sizeof(double), cudaMemcpyHostToDevice, s->stream));
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  s->profiling = true;
+  CK(cudaEventRecord(e0, s->stream));
+  int rc = enqueue_step(s);
+  CK(cudaEventRecord(e1, s->stream));
+  s->profiling = false;
+  CK(cudaStreamSynchronize(s->stream));
+  float acc[3] = {0.f, 0.f, 0.f};
+  int cnt[3] = {0, 0, 0};
+  for (size_t k = 0; k + 1 < s->prof_ev.size(); k += 2) {
+    float x = 0.f;
+    cudaEventElapsedTime(&x, s->prof_ev[k], s->prof_ev[k + 1]);
+    int c = s->prof_cls[k];
+    if (c >= 0 && c < 3) {
+      acc[c] += x;
+      cnt[c]++;
+    }
+  }
+  float tot = 0.f;
+  cudaEventElapsedTime(&tot, e0, e1);
+  for (auto e : s->prof_ev) cudaEventDestroy(e);
+  s->prof_ev.clear();
+  s->prof_cls.clear();
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  for (int c = 0; c < 3; ++c) {
+    ms[c] = acc[c];
+    if (launches) launches[c] = cnt[c];
+  }
+  ms[3] = tot;
+  CK(cudaMemcpy(s->h_ctl, s->ctl, sizeof(JacobiCtl), cudaMemcpyDeviceToHost));
+  for (int k = 0; k < s->n_solves && k < kMaxSolves; ++k) s->stats.jacobi_iters[k] = s->h_ctl->iters[k];
+  s->stats.n_solves = s->n_solves;
+  return s->h_ctl->status < 0 ? fail(SWM_ERR_WATCHDOG, "watchdog") : SWM_OK;
+}
+
+int swm_run(swm_handle s, double t_end, int n_outputs, int* n_steps, double* t_reached) {
+  if (!s || n_outputs < 1) return fail(SWM_ERR_PARAM, "invalid argument");
+  // timediscretization.f90:46-95 (I/O omitted)
+  double t = 0.0, dt_an = t_end / (double)n_outputs, t_an = t + dt_an;
+  int steps = 0, warn = 0;
+  if (t != t_end) {
+    for (;;) {
+      double dt_min;
+      int rc = swm_timestep(s, &dt_min);
+      if (rc < 0) return rc;
+      double a = dt_min < (t_an - t) ? dt_min : (t_an - t);
+      double b = dt_min < (t_end - t) ? dt_min : (t_end - t);
+      double dt = a < b ? a : b;
+      rc = swm_step(s, t, dt);
+      if (rc < 0) return rc;
+      if (rc > 0) warn = rc;
+      steps++;
+      t = t + dt;
+      if (fabs(t_an - t) < 1.0e-10) {
+        t_an = t_an + dt_an;
+        if (t_an > t_end) t_an = t_end;
+      }
+      if (fabs(t - t_end) < 1.0e-10) break;
+    }
+  }
+  if (n_steps) *n_steps = steps;
+  if (t_reached) *t_reached = t;
+  return warn;
+}
+
+int swm_get_stats(swm_handle s, swm_stats* out) {
+  if (!s || !out) return fail(SWM_ERR_PARAM, "null argument");
+  *out = s->stats;
+  return SWM_OK;
+}
+
+int swm_state_summary(swm_handle s, double* mass, double* min_h) {
+  if (!s) return fail(SWM_ERR_PARAM, "null handle");
+  if (!s->have_state) return fail(SWM_ERR_STATE, "no state set");
+  CK(cudaSetDevice(s->device));
+  CK(launch_summary(s->h, (int)s->N, s->summary, s->stream));
+  double res[2];
+  CK(cudaMemcpyAsync(res, s->summary, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  if (mass) *mass = res[0];
+  if (min_h) *min_h = res[1];
+  return SWM_OK;
+}
+
+const char* swm_last_error(void) { return g_last_error.c_str(); }
+
+const char* swm_strerror(int status) {
+  switch (status) {
+    case SWM_OK: return "ok";
+    case SWM_WARN_JACOBI_MAXITER: return "Jacobi not converged (maxIter reached)";
+    case SWM_ERR_PARAM: return "invalid parameter";
+    case SWM_ERR_CUDA: return "CUDA error";
+    case SWM_ERR_NAN: return "non-finite state";
+    case SWM_ERR_WATCHDOG: return "device watchdog expired";
+    case SWM_ERR_ALLOC: return "allocation failed";
+    case SWM_ERR_STATE: return "call out of order";
+    case SWM_ERR_UNSUPPORTED: return "unsupported on this device";
+    default: return "unknown status";
+  }
+}
+
+int swm_debug_rhs(swm_handle s, const double* U, double* Ut, double* FX, double* FY, double* S) {
+  if (!s || !U) return fail(SWM_ERR_PARAM, "null argument");
+  if (s->p.well_balanced && !s->have_wb) return fail(SWM_ERR_STATE, "WB state not set");
+  CK(cudaSetDevice(s->device));
+  const size_t nx = s->nx, ny = s->ny, N = s->N;
+  const size_t nfx = (nx + 1) * ny, nfy = nx * (ny + 1);
+  double *h = s->hbuf[1][0], *hu = s->hum[1], *hv = s->hvm[1];
+  int rc = upload_ghosted(s, U, h, hu, hv);
+  if (rc) return rc;
+  double *dfx = nullptr, *dfy = nullptr, *ds = nullptr;
+  CK(cudaMalloc(&dfx, 3 * nfx * sizeof(double)));
+  CK(cudaMalloc(&dfy, 3 * nfy * sizeof(double)));
+  CK(cudaMalloc(&ds, 3 * N * sizeof(double)));
+  RhsArgs a = make_rhs_args(s, h, hu, hv, 1);
+  a.fx_full = dfx;
+  a.fy_full = dfy;
+  a.s_full = ds;
+  cudaError_t e = launch_rhs(s, a);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);  // s->stream is non-blocking
+  std::vector<double> hfx(3 * nfx), hfy(3 * nfy), hs(3 * N), hut(N), hvt(N);
+  if (e == cudaSuccess) e = cudaMemcpy(hfx.data(), dfx, 3 * nfx * sizeof(double), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(hfy.data(), dfy, 3 * nfy * sizeof(double), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(hs.data(), ds, 3 * N * sizeof(double), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(hut.data(), s->fu[1], N * sizeof(double), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(hvt.data(), s->fv[1], N * sizeof(double), cudaMemcpyDeviceToHost);
+  cudaFree(dfx);
+  cudaFree(dfy);
+  cudaFree(ds);
+  if (e != cudaSuccess) return fail(SWM_ERR_CUDA, cudaGetErrorString(e));
+  // to the reference's column-major (3, ., .) layouts
+  for (size_t j = 0; j < ny; ++j)
+    for (size_t i = 0; i < nx; ++i) {
+      size_t c = j * nx + i;
+      if (Ut) {
+        Ut[3 * c] = 0.0;
+        Ut[3 * c + 1] = hut[c];
+        Ut[3 * c + 2] = hvt[c];
+      }
+      if (S)
+        for (int v = 0; v < 3; ++v) S[3 * c + v] = hs[v * N + c];
+    }
+  if (FX)
+    for (size_t j = 0; j < ny; ++j)
+      for (size_t f = 0; f <= nx; ++f)
+        for (int v = 0; v < 3; ++v) FX[3 * (j * (nx + 1) + f) + v] = hfx[v * nfx + j * (nx + 1) + f];
+  if (FY)
+    for (size_t f = 0; f <= ny; ++f)
+      for (size_t i = 0; i < nx; ++i)
+        for (int v = 0; v < 3; ++v) FY[3 * (f * nx + i) + v] = hfy[v * nfy + f * nx + i];
+  return SWM_OK;
+}
+
+int swm_debug_jacobi(swm_handle s, const double* mass, const double* diag, const double* rhs,
+                     double* sol, int* iters) {
+  if (!s || !mass || !diag || !rhs || !sol) return fail(SWM_ERR_PARAM, "null argument");
+  CK(cudaSetDevice(s->device));
+  const size_t N = s->N;
+  const bool csr = s->p.solver == SWM_SOLVER_CSR;
+  double* b = s->hbuf[1][0];
+  double* out = s->hbuf[1][1];
+  CK(cudaMemcpy(b, rhs, N * sizeof(double), cudaMemcpyHostToDevice));
+  if (csr) {
+    CK(cudaMemcpy(s->csr_mass, mass, 5 * N * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(s->csr_diag, diag, N * sizeof(double), cudaMemcpyHostToDevice));
+  } else {
+    std::vector<double> pl(5 * N);
+    for (size_t k = 0; k < N; ++k) {
+      pl[k] = mass[5 * k + 0];
+      pl[N + k] = mass[5 * k + 1];
+      pl[2 * N + k] = mass[5 * k + 3];
+      pl[3 * N + k] = mass[5 * k + 4];
+      pl[4 * N + k] = diag[k];
+    }
+    CK(cudaMemcpy(s->cS, pl.data(), N * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(s->cW, pl.data() + N, N * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(s->cE, pl.data() + 2 * N, N * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(s->cN, pl.data() + 3 * N, N * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(s->cD, pl.data() + 4 * N, N * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  CK(cudaMemset(&s->ctl->iters[0], 0, sizeof(int) * (kMaxSolves + 1)));
+  JacobiArgs ja{};
+  ja.nx = s->nx;
+  ja.ny = s->ny;
+  ja.solve_idx = 0;
+  ja.maxiter = s->p.jacobi_maxiter;
+  fill_thresh(s, ja.thresh);
+  ja.b = b;
+  ja.cS = s->cS;
+  ja.cW = s->cW;
+  ja.cE = s->cE;
+  ja.cN = s->cN;
+  ja.cD = s->cD;
+  ja.rowstart = s->rowstart;
+  ja.cols = s->cols;
+  ja.mass = s->csr_mass;
+  ja.diag = s->csr_diag;
+  ja.xa = s->xa;
+  ja.xb = s->xb;
+  ja.out = out;
+  ja.ctl = s->ctl;
+  ja.block = jacobi_block_of(s->p);
+  ja.spin_limit = 1LL << 26;
+  CK(launch_jacobi(ja, csr, s->jac_blocks, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  CK(cudaMemcpy(sol, out, N * sizeof(double), cudaMemcpyDeviceToHost));
+  JacobiCtl c;
+  CK(cudaMemcpy(&c, s->ctl, sizeof(JacobiCtl), cudaMemcpyDeviceToHost));
+  if (iters) *iters = c.iters[0];
+  if (c.status < 0) return fail(SWM_ERR_WATCHDOG, "Jacobi grid barrier watchdog expired");
+  return c.status == 1 ? SWM_WARN_JACOBI_MAXITER : SWM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,283 @@
+// swm_device.cuh -- device building blocks of the mPDeC5 time step (sm_100a).
+//
+// The three precision forms share this code:
+//   EXACT  (FP64, translation unit built with -fmad=false): the reference's
+//          expression order and IEEE divisions, so that results match the CPU
+//          restatement of the Fortran bit for bit where no libm call is involved;
+//   FAST   (FP64, FMA contraction): WENO weights use one reciprocal per
+//          smoothness indicator and one per Gauss point instead of six
+//          divisions per point;
+//   SPLIT  (FP32 WENO on deviations from the cell value, FP64 everywhere else).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#ifndef SWM_EXACT
+#define SWM_EXACT 0
+#endif
+
+namespace swm {
+
+// finitevolume_vars.f90:96-106
+constexpr double kMinDepth = 1.0e-6;
+constexpr double kWenoEps = 1.0e-24;
+// FP32 WENO uses eps = 1e-18: (1e-24)^2 underflows to 0 in FP32, which would turn
+// a flat stencil's weights into inf/inf.  (1e-18)^2 = 1e-36 is a normal float.
+constexpr float kWenoEpsF = 1.0e-18f;
+constexpr double kWLobatto = 1. / 12.;
+
+// Bathymetry kinds (swm.h SWM_BATHY_*)
+enum { BATHY_FLAT = 0, BATHY_SINCOS = 1, BATHY_BUMP = 2, BATHY_GAUSS = 3 };
+
+struct Grid {
+  int nx, ny;
+  double x0, y0;
+  double dx, dy;
+  double g;
+  int bathy;
+  double bp[5];  // Gaussian A, ax, cx, ay, cy
+  double qn[4];  // Gauss nodes on [-1/2, 1/2] (mesh.f90:128-129)
+  double qw[4];  // Gauss weights (mesh.f90:127)
+  double wgp[4][4];
+};
+
+__device__ __forceinline__ int wrap(int i, int n) {
+  int r = i % n;
+  return r < 0 ? r + n : r;
+}
+__device__ __forceinline__ double dmax(double a, double b) { return (a > b) ? a : b; }
+__device__ __forceinline__ double dmin(double a, double b) { return (a < b) ? a : b; }
+
+__device__ __forceinline__ double rcp_(double x) { return 1.0 / x; }
+__device__ __forceinline__ float rcp_(float x) { return __fdividef(1.0f, x); }
+
+template <typename T>
+__device__ __forceinline__ T weno_eps();
+template <>
+__device__ __forceinline__ double weno_eps<double>() { return kWenoEps; }
+template <>
+__device__ __forceinline__ float weno_eps<float>() { return kWenoEpsF; }
+
+// Smoothness indicators (reconstruction.f90:699-704 and :1024-1029), squared with eps.
+// EXACT keeps the reference's expanded quadratic forms.  The other forms use the
+// identical sums of squares, e.g. 3*beta1 = 4a^2-19ab+25b^2+11ac-31bc+10c^2 =
+// 3*(13/12 (a-2b+c)^2 + 1/4 (a-4b+3c)^2): non-negative by construction and free of
+// the cancellation of the expanded form, which in FP32 can drive eps+beta to zero
+// (and the weights to inf/inf) on nearly constant stencils.
+template <typename T, bool EXACT>
+__device__ __forceinline__ void weno_d(T qm2, T qm1, T q0, T qp1, T qp2, T& d1, T& d2, T& d3) {
+  T beta1, beta2, beta3;
+  if (EXACT) {
+    beta1 = (T(1.0) / T(3.0)) * (T(4.0) * qm2 * qm2 - T(19.0) * qm2 * qm1 + T(25.0) * qm1 * qm1 +
+                                 T(11.0) * qm2 * q0 - T(31.0) * qm1 * q0 + T(10.0) * q0 * q0);
+    beta2 = (T(1.0) / T(3.0)) * (T(4.0) * qm1 * qm1 - T(13.0) * qm1 * q0 + T(13.0) * q0 * q0 +
+                                 T(5.0) * qm1 * qp1 - T(13.0) * q0 * qp1 + T(4.0) * qp1 * qp1);
+    beta3 = (T(1.0) / T(3.0)) * (T(10.0) * q0 * q0 - T(31.0) * q0 * qp1 + T(25.0) * qp1 * qp1 +
+                                 T(11.0) * q0 * qp2 - T(19.0) * qp1 * qp2 + T(4.0) * qp2 * qp2);
+  } else {
+    const T c13 = T(13.0) / T(12.0), c4 = T(0.25);
+    T s1 = qm2 - T(2.0) * qm1 + q0, r1 = qm2 - T(4.0) * qm1 + T(3.0) * q0;
+    T s2 = qm1 - T(2.0) * q0 + qp1, r2 = qm1 - qp1;
+    T s3 = q0 - T(2.0) * qp1 + qp2, r3 = T(3.0) * q0 - T(4.0) * qp1 + qp2;
+    beta1 = c13 * (s1 * s1) + c4 * (r1 * r1);
+    beta2 = c13 * (s2 * s2) + c4 * (r2 * r2);
+    beta3 = c13 * (s3 * s3) + c4 * (r3 * r3);
+  }
+  T t1 = weno_eps<T>() + beta1, t2 = weno_eps<T>() + beta2, t3 = weno_eps<T>() + beta3;
+  d1 = t1 * t1;
+  d2 = t2 * t2;
+  d3 = t3 * t3;
+}
+
+// Nonlinear combination of one reconstruction point.
+//  EXACT: omega_k = alpha_k/(alpha1+alpha2+alpha3), alpha_k = gamma_k/d_k
+//         (reconstruction.f90:716-728), literal order.
+//  else : the same weights from shared reciprocals i_k = 1/d_k.
+template <typename T, bool EXACT>
+__device__ __forceinline__ T weno_point(T g1, T g2, T g3, T d1, T d2, T d3, T i1, T i2, T i3, T W1,
+                                        T W2, T W3) {
+  if (EXACT) {
+    T a1 = g1 / d1, a2 = g2 / d2, a3 = g3 / d3;
+    return a1 / (a1 + a2 + a3) * W1 + a2 / (a1 + a2 + a3) * W2 + a3 / (a1 + a2 + a3) * W3;
+  } else {
+    T a1 = g1 * i1, a2 = g2 * i2, a3 = g3 * i3;
+    return (a1 * W1 + a2 * W2 + a3 * W3) * rcp_(a1 + a2 + a3);
+  }
+}
+
+// WENO5_FirstSweep (reconstruction.f90:673-755): cell-face means at x_{i-1/2}, x_{i+1/2}.
+template <typename T, bool EXACT>
+__device__ __forceinline__ void weno5_first(T qm2, T qm1, T q0, T qp1, T qp2, T& wm, T& wp) {
+  T d1, d2, d3, i1 = T(0), i2 = T(0), i3 = T(0);
+  weno_d<T, EXACT>(qm2, qm1, q0, qp1, qp2, d1, d2, d3);
+  if (!EXACT) {
+    i1 = rcp_(d1);
+    i2 = rcp_(d2);
+    i3 = rcp_(d3);
+  }
+  const T s6 = T(1.0) / T(6.0);
+  T W1 = s6 * (-qm2 + T(5.0) * qm1 + T(2.0) * q0);
+  T W2 = s6 * (T(2.0) * qm1 + T(5.0) * q0 - qp1);
+  T W3 = s6 * (T(11.0) * q0 - T(7.0) * qp1 + T(2.0) * qp2);
+  wm = weno_point<T, EXACT>(T(3.0) / T(10.0), T(3.0) / T(5.0), T(1.0) / T(10.0), d1, d2, d3, i1, i2,
+                            i3, W1, W2, W3);
+  W1 = s6 * (T(2.0) * qm2 - T(7.0) * qm1 + T(11.0) * q0);
+  W2 = s6 * (-qm1 + T(5.0) * q0 + T(2.0) * qp1);
+  W3 = s6 * (T(2.0) * q0 + T(5.0) * qp1 - qp2);
+  wp = weno_point<T, EXACT>(T(1.0) / T(10.0), T(3.0) / T(5.0), T(3.0) / T(10.0), d1, d2, d3, i1, i2,
+                            i3, W1, W2, W3);
+}
+
+// WENO5_SecondSweep (reconstruction.f90:999-1136): values at the 4 Gauss nodes.
+// Linear weights and sub-stencil coefficients are the reference's tabulated
+// constants (generated offline by weno-weights/WENO_double.m); the reference's
+// 0.0*Q(k) terms are omitted (they only change the sign of an exact zero).
+template <typename T, bool EXACT>
+__device__ __forceinline__ void weno5_second(T qm2, T qm1, T q0, T qp1, T qp2, T w[4]) {
+  T d1, d2, d3, i1 = T(0), i2 = T(0), i3 = T(0);
+  weno_d<T, EXACT>(qm2, qm1, q0, qp1, qp2, d1, d2, d3);
+  if (!EXACT) {
+    i1 = rcp_(d1);
+    i2 = rcp_(d2);
+    i3 = rcp_(d3);
+  }
+  T W1, W2, W3;
+  W1 = T(-0.1642562761719537) * qm2 + T(0.7590807081409336) * qm1 + T(0.4051755680310201) * q0;
+  W2 = T(0.2663118796250726) * qm1 + T(0.8979443965468811) * q0 - T(0.1642562761719537) * qp1;
+  W3 = T(1.6968800354220990) * q0 - T(0.9631919150471715) * qp1 + T(0.2663118796250726) * qp2;
+  w[0] = weno_point<T, EXACT>(T(0.2658420974778319), T(0.6112504900322486), T(0.1229074124899195),
+                              d1, d2, d3, i1, i2, i3, W1, W2, W3);
+  W1 = T(-0.1122135388132497) * qm2 + T(0.3944175994189276) * qm1 + T(0.7177959393943222) * q0;
+  W2 = T(0.0577769829791784) * qm1 + T(1.0544365558340714) * q0 - T(0.1122135388132497) * qp1;
+  W3 = T(1.2277675047716066) * q0 - T(0.2855444877507849) * qp1 + T(0.0577769829791784) * qp2;
+  w[1] = weno_point<T, EXACT>(T(0.1281641584355059), T(0.5219691498503563), T(0.3498666917141379),
+                              d1, d2, d3, i1, i2, i3, W1, W2, W3);
+  W1 = T(0.0577769829791784) * qm2 - T(0.2855444877507849) * qm1 + T(1.2277675047716066) * q0;
+  W2 = T(-0.1122135388132497) * qm1 + T(1.0544365558340714) * q0 + T(0.0577769829791784) * qp1;
+  W3 = T(0.7177959393943222) * q0 + T(0.3944175994189276) * qp1 - T(0.1122135388132497) * qp2;
+  w[2] = weno_point<T, EXACT>(T(0.3498666917141379), T(0.5219691498503563), T(0.1281641584355059),
+                              d1, d2, d3, i1, i2, i3, W1, W2, W3);
+  W1 = T(0.2663118796250726) * qm2 - T(0.9631919150471715) * qm1 + T(1.6968800354220990) * q0;
+  W2 = T(-0.1642562761719537) * qm1 + T(0.8979443965468811) * q0 + T(0.2663118796250726) * qp1;
+  W3 = T(0.4051755680310201) * q0 + T(0.7590807081409336) * qp1 - T(0.1642562761719537) * qp2;
+  w[3] = weno_point<T, EXACT>(T(0.1229074124899195), T(0.6112504900322486), T(0.2658420974778319),
+                              d1, d2, d3, i1, i2, i3, W1, W2, W3);
+}
+
+// ConsToPrim (equation.f90:912-945)
+__device__ __forceinline__ void cons_to_prim(double h, double hu, double hv, double& u, double& v) {
+  double ht = h + kMinDepth / h;
+  u = hu / ht;
+  v = hv / ht;
+}
+
+// Rusanov flux in the face-normal frame: EvaluateFlux1D + WaveSpeeds1D +
+// RiemannSolverByRusanov (equation.f90:988-1106).  (hn = normal velocity,
+// ht = tangential); the reference's rotations by n=(1,0)/(0,1) and t=(0,1)/(-1,0)
+// multiply by exact 0 and +-1, so an x face passes (h,u,v) and a y face (h,v,u)
+// with the tangential component mapped back.
+__device__ __forceinline__ void rusanov(double g, double hL, double nL, double tL, double hR,
+                                        double nR, double tR, double& F0, double& F1, double& F2) {
+  double FL0 = hL * nL;
+  double FL1 = hL * (nL * nL) + 0.5 * g * (hL * hL);
+  double FL2 = hL * nL * tL;
+  double FR0 = hR * nR;
+  double FR1 = hR * (nR * nR) + 0.5 * g * (hR * hR);
+  double FR2 = hR * nR * tR;
+  double fastL = nL + sqrt(g * hL), fastR = nR + sqrt(g * hR);
+  double lam = dmax(fabs(fastL), fabs(fastR));
+  F0 = 0.5 * ((FL0 + FR0) - lam * (hR - hL));
+  F1 = 0.5 * ((FL1 + FR1) - lam * (hR * nR - hL * nL));
+  F2 = 0.5 * ((FL2 + FR2) - lam * (hR * tR - hL * tL));
+}
+
+// Positivity limiter on the 4 face values of h of one cell
+// (finitevolume.f90:671-691, identical for x and y).
+__device__ __forceinline__ void limit_h(const Grid& gr, double Vc, double wm[4], double wp[4]) {
+  double alpha = 0., beta = 0.;
+#pragma unroll
+  for (int g = 0; g < 4; ++g) {
+    alpha = alpha + gr.qw[g] * wm[g];
+    beta = beta + gr.qw[g] * wp[g];
+  }
+  double csi = (Vc - kWLobatto * alpha - kWLobatto * beta) / (1. - 2. * kWLobatto);
+#pragma unroll
+  for (int g = 0; g < 4; ++g) {
+    double mmin = csi;
+    if (wm[g] < mmin) mmin = wm[g];
+    if (wp[g] < mmin) mmin = wp[g];
+    double theta;
+    if (Vc == mmin)
+      theta = 1.;
+    else
+      theta = dmin(1., fabs((Vc - kMinDepth) / (Vc - mmin)));
+    wp[g] = Vc + theta * (wp[g] - Vc);
+    wm[g] = Vc + theta * (wm[g] - Vc);
+  }
+}
+
+// The same limiter on deviations d = W - Vc (split form): csi - Vc =
+// -(wL a' + wL b')/(1 - 2 wL) with a' = sum w_g dM_g, b' = sum w_g dP_g; theta is
+// formed in FP64 so that the limited depth V + theta*d stays >= MIN_DEPTH up to
+// FP64 rounding.
+__device__ __forceinline__ void limit_h_dev(const Grid& gr, double Vc, const float dm[4],
+                                            const float dp[4], double wm[4], double wp[4]) {
+  double alpha = 0., beta = 0.;
+#pragma unroll
+  for (int g = 0; g < 4; ++g) {
+    alpha = alpha + gr.qw[g] * (double)dm[g];
+    beta = beta + gr.qw[g] * (double)dp[g];
+  }
+  double csi = -(kWLobatto * alpha + kWLobatto * beta) / (1. - 2. * kWLobatto);
+#pragma unroll
+  for (int g = 0; g < 4; ++g) {
+    double mmin = csi;
+    if ((double)dm[g] < mmin) mmin = (double)dm[g];
+    if ((double)dp[g] < mmin) mmin = (double)dp[g];
+    double theta;
+    if (mmin == 0.)
+      theta = 1.;
+    else
+      theta = dmin(1., fabs((Vc - kMinDepth) / mmin));
+    wp[g] = Vc + theta * (double)dp[g];
+    wm[g] = Vc + theta * (double)dm[g];
+  }
+}
+
+// Bathymetry gradient (equation.f90:451-509; flag 3 is the Gaussian used by the
+// benchmark cases).
+__device__ __forceinline__ void bathy_grad(const Grid& gr, double x, double y, double& bx,
+                                           double& by) {
+  const double PI = 3.141592653589793;  // ACOS(-1.0) in FP64
+  bx = 0.;
+  by = 0.;
+  if (gr.bathy == BATHY_SINCOS) {
+    bx = 0.1 * 2. * PI * cos(2. * PI * x) * cos(2. * PI * y);
+    by = -(0.1 * 2. * PI * sin(2. * PI * x) * sin(2. * PI * y));
+  } else if (gr.bathy == BATHY_BUMP) {
+    double r2 = x * x + y * y;
+    if (r2 < 1) {
+      double d = 1.0 - r2;
+      double e = exp(1.0 - 1.0 / d);
+      bx = -(2.0 * x / (d * d) * e);
+      by = -(2.0 * y / (d * d) * e);
+    }
+  } else if (gr.bathy == BATHY_GAUSS) {
+    double dxv = x - gr.bp[2], dyv = y - gr.bp[4];
+    double e = exp(-(gr.bp[1] * (dxv * dxv) + gr.bp[3] * (dyv * dyv)));
+    double B = gr.bp[0] * e;
+    bx = (-2.0 * gr.bp[1] * dxv) * B;
+    by = (-2.0 * gr.bp[3] * dyv) * B;
+  }
+}
+
+// x (d=0) or y (d=1) coordinate of Gauss node q of cell index c (0-based),
+// mesh.f90:64,70,142: node = x0 + REAL(ii)*dx; bary = node + 0.5 dx; gp = bary + qn dx.
+__device__ __forceinline__ double gp_coord(const Grid& gr, int d, int c, int q) {
+  double x0 = d ? gr.y0 : gr.x0, h = d ? gr.dy : gr.dx;
+  double node = x0 + ((double)c) * h;
+  double bary = node + 0.5 * h;
+  return bary + gr.qn[q] * h;
+}
+
+}  // namespace swm

@@ -1,0 +1,633 @@
+// swm_kernels.cu -- memory-bound kernels of the mPDeC5 step (sm_100a).
+// Built with -fmad=false: every FP64 expression here rounds exactly as the
+// reference's source order does (no contraction), which makes the Patankar
+// matrix and the Jacobi iterates bit-identical to the CPU restatement given the
+// same fluxes, and the CSR and matrix-free solvers bit-identical to each other.
+#include <cooperative_groups.h>
+
+#include <cstdio>
+
+#include "swm_kernels.cuh"
+
+namespace swm {
+
+// ---------------------------------------------------------------------------
+// Residual limbs: |dx| in units of 2^-100 as three 40-bit integers.
+// Scaling by powers of two and flooring are exact in FP64, so the split is exact
+// (apart from truncation below 2^-100) and the integer sum is order-independent.
+// ---------------------------------------------------------------------------
+__host__ __device__ inline void residual_limbs(double v, unsigned long long& l2,
+                                               unsigned long long& l1, unsigned long long& l0) {
+  const unsigned long long m40 = (1ull << 40) - 1;
+  if (!(v < 1048576.0)) {  // >= 2^20 or NaN: saturate (never converged)
+    l2 = m40;
+    l1 = m40;
+    l0 = m40;
+    return;
+  }
+  double x = v * 0x1p100;
+  double q2 = floor(x * 0x1p-80);
+  double r = x - q2 * 0x1p80;
+  double q1 = floor(r * 0x1p-40);
+  double r0 = r - q1 * 0x1p40;
+  l2 = (unsigned long long)q2;
+  l1 = (unsigned long long)q1;
+  l0 = (unsigned long long)floor(r0);
+}
+
+void residual_limbs_host(double v, unsigned long long out[3]) {
+  unsigned long long a, b, c;
+  residual_limbs(v, a, b, c);
+  out[0] = a;
+  out[1] = b;
+  out[2] = c;
+}
+
+// total <= thresh for sums of limbs (each sum < 2^64): normalise carries, compare.
+__device__ __forceinline__ bool limbs_le(unsigned long long s2, unsigned long long s1,
+                                         unsigned long long s0, const unsigned long long* t) {
+  const unsigned long long m40 = (1ull << 40) - 1;
+  s1 += s0 >> 40;
+  s0 &= m40;
+  s2 += s1 >> 40;
+  s1 &= m40;
+  if (s2 != t[0]) return s2 < t[0];
+  if (s1 != t[1]) return s1 < t[1];
+  return s0 <= t[2];
+}
+
+__device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// ---------------------------------------------------------------------------
+// TimeStep (equation.f90:791-837): LambdaMaxX/Y = max |u + sqrt(g h)|, |v + sqrt(g h)|
+// ---------------------------------------------------------------------------
+__global__ void dt_kernel(const DtArgs a) {
+  const int n = a.nx * a.ny;
+  double lx = 0.0, ly = 0.0;
+  int bad = 0;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    double h = a.h[k], hu = a.hu[k], hv = a.hv[k], u, v;
+    if (!(h >= 0.0) || !isfinite(h) || !isfinite(hu) || !isfinite(hv)) bad = 1;
+    cons_to_prim(h, hu, hv, u, v);
+    double c = sqrt(a.g * h);
+    lx = dmax(lx, fabs(u + c));
+    ly = dmax(ly, fabs(v + c));
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    lx = dmax(lx, __shfl_down_sync(0xffffffffu, lx, o));
+    ly = dmax(ly, __shfl_down_sync(0xffffffffu, ly, o));
+  }
+  bad = __any_sync(0xffffffffu, bad);
+  if ((threadIdx.x & 31) == 0) {
+    // non-negative doubles order like their bit patterns
+    atomicMax(&a.lam[0], (unsigned long long)__double_as_longlong(lx));
+    atomicMax(&a.lam[1], (unsigned long long)__double_as_longlong(ly));
+    if (bad) atomicOr(a.bad, 1);
+  }
+}
+
+cudaError_t launch_dt(const DtArgs& a, cudaStream_t s) {
+  int n = a.nx * a.ny;
+  int blocks = (n + 255) / 256;
+  if (blocks > 148 * 8) blocks = 148 * 8;
+  dt_kernel<<<blocks, 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Layout conversion between the reference's ghosted array U(1:3,-2:nx+3,-2:ny+3)
+// and the device planes [ny][nx].
+// ---------------------------------------------------------------------------
+__global__ void ghosted_to_planes_kernel(const double* __restrict__ G, int nx, int ny, double* h,
+                                         double* hu, double* hv) {
+  int n = nx * ny;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    int i = k % nx, j = k / nx;
+    size_t g = 3 * ((size_t)(i + 3) + (size_t)(nx + 6) * (j + 3));
+    h[k] = G[g];
+    hu[k] = G[g + 1];
+    hv[k] = G[g + 2];
+  }
+}
+
+// Ghost frame filled periodically (the values BoundaryConditions would write,
+// equation.f90:556-776); Vg (nullable) = ConsToPrim on the whole array.
+__global__ void planes_to_ghosted_kernel(const double* h, const double* hu, const double* hv,
+                                         int nx, int ny, double* G, double* Vg) {
+  int W = nx + 6, n = W * (ny + 6);
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    int gi = k % W - 3, gj = k / W - 3;
+    int i = wrap(gi, nx), j = wrap(gj, ny);
+    size_t s = (size_t)j * nx + i;
+    double a = h[s], b = hu[s], c = hv[s];
+    G[3 * (size_t)k] = a;
+    G[3 * (size_t)k + 1] = b;
+    G[3 * (size_t)k + 2] = c;
+    if (Vg) {
+      double u, v;
+      cons_to_prim(a, b, c, u, v);
+      Vg[3 * (size_t)k] = a;
+      Vg[3 * (size_t)k + 1] = u;
+      Vg[3 * (size_t)k + 2] = v;
+    }
+  }
+}
+
+cudaError_t launch_ghosted_to_planes(const double* G, int nx, int ny, double* h, double* hu,
+                                     double* hv, cudaStream_t s) {
+  int n = nx * ny, blocks = (n + 255) / 256;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  ghosted_to_planes_kernel<<<blocks, 256, 0, s>>>(G, nx, ny, h, hu, hv);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_planes_to_ghosted(const double* h, const double* hu, const double* hv, int nx,
+                                     int ny, double* G, double* Vg, cudaStream_t s) {
+  int n = (nx + 6) * (ny + 6), blocks = (n + 255) / 256;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  planes_to_ghosted_kernel<<<blocks, 256, 0, s>>>(h, hu, hv, nx, ny, G, Vg);
+  return cudaGetLastError();
+}
+
+// mass = sum h (per-block partials in fixed order, then one block), min h.
+__global__ void summary_kernel(const double* h, int n, double* part_sum, double* part_min) {
+  __shared__ double ss[256], sm[256];
+  double s = 0.0, m = 1e300;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    s += h[k];
+    m = dmin(m, h[k]);
+  }
+  ss[threadIdx.x] = s;
+  sm[threadIdx.x] = m;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      ss[threadIdx.x] += ss[threadIdx.x + o];
+      sm[threadIdx.x] = dmin(sm[threadIdx.x], sm[threadIdx.x + o]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    part_sum[blockIdx.x] = ss[0];
+    part_min[blockIdx.x] = sm[0];
+  }
+}
+__global__ void summary_final_kernel(const double* ps, const double* pm, int nb, double* out) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    double s = 0.0, m = 1e300;
+    for (int b = 0; b < nb; ++b) {
+      s += ps[b];
+      m = dmin(m, pm[b]);
+    }
+    out[0] = s;
+    out[1] = m;
+  }
+}
+cudaError_t launch_summary(const double* h, int n, double* out, cudaStream_t s) {
+  // out must have room for 2 + 2*256 doubles (partials after the result)
+  const int nb = 256;
+  summary_kernel<<<nb, 256, 0, s>>>(h, n, out + 2, out + 2 + nb);
+  summary_final_kernel<<<1, 32, 0, s>>>(out + 2, out + 2 + nb, nb, out);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Stage combination + Patankar assembly for substep m
+//   Ua(m,2:3) = Ua(1,2:3) + sum_r dt theta(m,r) FUp(r,2:3)   timediscretization.f90:539-543
+//   Mass/Diagonal of MODIFIED_PATANKAR_MATRIX_INVERSION       timediscretization.f90:795-885
+// P/D entries are rebuilt from the stored mass fluxes with the same operations
+// UpdateTimeDerivative uses (finitevolume.f90:500-523).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double patankar_div(double prod, double h) {
+  // timediscretization.f90:913-924
+  if (h < kMinDepth) return 0.;
+  return 2. * h * prod / (h * h + dmax(h * h, kMinDepth));
+}
+
+__device__ __forceinline__ double hp_read(const AssembleArgs& a, int m, int i, int j) {
+  // m, i, j 0-based
+  if (a.msteps == 2 && a.compat2) {
+    long long L = (long long)m + 2LL * ((long long)i + (long long)a.nx * j);
+    int s = (int)(L % 4);
+    long long c = L / 4;
+    int ic = (int)(c % a.nx), jc = (int)(c / a.nx);
+    if (s >= 2) return 0.0;  // Up(3:4,...) are never written by mPDeC2
+    return a.hp[s][(size_t)jc * a.nx + ic];
+  }
+  return a.hp[m][(size_t)j * a.nx + i];
+}
+
+__global__ void assemble_kernel(const AssembleArgs a, bool csr) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y;
+  if (i >= a.nx || j >= a.ny) return;
+  const int nx = a.nx, ny = a.ny;
+  const size_t k = (size_t)j * nx + i;
+  const double dt = *a.dt;
+  const int ms = a.msteps;
+  // explicit momentum
+  double au = a.hu_n[k], av = a.hv_n[k];
+  for (int r = 0; r < ms; ++r) {
+    au = au + dt * a.theta[r] * a.fu[r][k];
+    av = av + dt * a.theta[r] * a.fv[r][k];
+  }
+  a.hu_out[k] = au;
+  a.hv_out[k] = av;
+  // Patankar weights
+  const int m = a.m - 1;
+  const double hK = hp_read(a, m, i, j);
+  const int ni[4] = {i, wrap(i - 1, nx), wrap(i + 1, nx), i};
+  const int nj[4] = {wrap(j - 1, ny), j, j, wrap(j + 1, ny)};
+  double M[4] = {0., 0., 0., 0.};
+  double D = 1.;
+#pragma unroll
+  for (int nb = 0; nb < 4; ++nb) {
+    const double hL = hp_read(a, m, ni[nb], nj[nb]);
+    for (int r = 0; r < ms; ++r) {
+      double f, P, Q;
+      if (nb == 0) {
+        f = a.fym[r][(size_t)j * nx + i];
+        P = dmax(f, 0.) / a.dy;
+        Q = -dmin(f, 0.) / a.dy;
+      } else if (nb == 1) {
+        f = a.fxm[r][(size_t)j * (nx + 1) + i];
+        P = dmax(f, 0.) / a.dx;
+        Q = -dmin(f, 0.) / a.dx;
+      } else if (nb == 2) {
+        f = -a.fxm[r][(size_t)j * (nx + 1) + i + 1];
+        P = dmax(f, 0.) / a.dx;
+        Q = -dmin(f, 0.) / a.dx;
+      } else {
+        f = -a.fym[r][(size_t)(j + 1) * nx + i];
+        P = dmax(f, 0.) / a.dy;
+        Q = -dmin(f, 0.) / a.dy;
+      }
+      const double th = a.theta[r];
+      if (th > 0.) {
+        M[nb] = M[nb] - dt * th * (patankar_div(P, hL));
+        D = D + dt * th * (patankar_div(Q, hK));
+      } else {
+        D = D - dt * th * (patankar_div(P, hK));
+        M[nb] = M[nb] + dt * th * (patankar_div(Q, hL));
+      }
+    }
+  }
+  if (csr) {
+    // CSR slots S, W, C, E, N of row K (finitevolume.f90:234-261)
+    double* mv = a.csr_mass + 5 * k;
+    mv[0] = M[0];
+    mv[1] = M[1];
+    mv[2] = 0.;
+    mv[3] = M[2];
+    mv[4] = M[3];
+    a.csr_diag[k] = D;
+  } else {
+    a.cS[k] = M[0];
+    a.cW[k] = M[1];
+    a.cE[k] = M[2];
+    a.cN[k] = M[3];
+    a.cD[k] = D;
+  }
+  if (a.rhs_out) a.rhs_out[k] = hp_read(a, 0, i, j);  // rhs = hp(1,.) (timediscretization.f90:887)
+}
+
+cudaError_t launch_assemble(const AssembleArgs& a, bool csr, cudaStream_t s) {
+  dim3 blk(128), grd((a.nx + 127) / 128, a.ny);
+  assemble_kernel<<<grd, blk, 0, s>>>(a, csr);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Jacobi (jacobi_iteration.f90:52-87): x^{k+1} = (b - L x^k)/D from x^0 = b,
+// residual mean|x^{k+1}-x^k|, stop when <= tol or at maxIter.
+// One cooperative persistent launch per solve; passes separated by a bounded
+// grid barrier; the stop decision is taken identically by every CTA from the
+// integer residual sums.
+// ---------------------------------------------------------------------------
+__device__ bool grid_barrier(JacobiCtl* ctl, long long spin_limit, int* s_ok) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned int* vgen = &ctl->bar_gen;
+    unsigned int gen = *vgen;
+    __threadfence();
+    unsigned int arrived = atomicAdd(&ctl->bar_count, 1u);
+    int ok = 1;
+    if (arrived == gridDim.x - 1) {
+      atomicExch(&ctl->bar_count, 0u);
+      __threadfence();
+      atomicAdd(&ctl->bar_gen, 1u);
+    } else {
+      long long spins = 0;
+      while (*vgen == gen) {
+        if (++spins > spin_limit) {
+          ok = 0;
+          atomicExch(&ctl->status, -4);
+          break;
+        }
+        __nanosleep(40);
+      }
+    }
+    __threadfence();
+    *s_ok = ok;
+  }
+  __syncthreads();
+  return *s_ok != 0;
+}
+
+// Stencil tile geometry
+constexpr int JBX = 64, JBY = 16, JNT = 512;
+
+template <int TB>
+struct JTile {
+  static constexpr int HX = JBX + 2 * TB, HY = JBY + 2 * TB, HN = HX * HY;
+  static constexpr size_t bytes = sizeof(double) * 8 * HN;
+};
+
+__device__ __forceinline__ void acc_add(unsigned long long* s_acc_t, double v) {
+  unsigned long long l2, l1, l0;
+  residual_limbs(v, l2, l1, l0);
+  l2 = warp_sum_u64(l2);
+  l1 = warp_sum_u64(l1);
+  l0 = warp_sum_u64(l0);
+  if ((threadIdx.x & 31) == 0) {
+    if (l2) atomicAdd(&s_acc_t[0], l2);
+    if (l1) atomicAdd(&s_acc_t[1], l1);
+    if (l0) atomicAdd(&s_acc_t[2], l0);
+  }
+}
+
+// One stencil pass of Tp <= TB sweeps over every tile of this CTA.
+template <int TB>
+__device__ void stencil_pass(const JacobiArgs& a, const double* xin, double* xout, int Tp,
+                             bool first, unsigned long long (*s_acc)[3], double* sm) {
+  using G = JTile<TB>;
+  constexpr int HX = G::HX, HY = G::HY, HN = G::HN;
+  double* sS = sm;
+  double* sW = sS + HN;
+  double* sE = sW + HN;
+  double* sN = sE + HN;
+  double* sD = sN + HN;
+  double* sB = sD + HN;
+  double* x0 = sB + HN;
+  double* x1 = x0 + HN;
+  const int nx = a.nx, ny = a.ny;
+  const int tx = (nx + JBX - 1) / JBX, ty = (ny + JBY - 1) / JBY;
+  for (int tile = blockIdx.x; tile < tx * ty; tile += gridDim.x) {
+    const int i0 = (tile % tx) * JBX, j0 = (tile / tx) * JBY;
+    for (int it = threadIdx.x; it < HN; it += JNT) {
+      int lx = it % HX, ly = it / HX;
+      int gi = wrap(i0 - TB + lx, nx), gj = wrap(j0 - TB + ly, ny);
+      size_t g = (size_t)gj * nx + gi;
+      sS[it] = a.cS[g];
+      sW[it] = a.cW[g];
+      sE[it] = a.cE[g];
+      sN[it] = a.cN[g];
+      sD[it] = a.cD[g];
+      sB[it] = a.b[g];
+      x0[it] = __ldcg(&xin[g]);
+    }
+    __syncthreads();
+    if (first) {  // initial residual mean|0 - b| (jacobi_iteration.f90:69)
+      static_assert((JBX * JBY) % JNT == 0, "uniform trip count for the warp reductions");
+      for (int it = threadIdx.x; it < JBX * JBY; it += JNT) {
+        int lx = it % JBX + TB, ly = it / JBX + TB;
+        int gi = i0 + lx - TB, gj = j0 + ly - TB;
+        double v = (gi < nx && gj < ny) ? fabs(0. - sB[ly * HX + lx]) : 0.;
+        acc_add(s_acc[0], v);
+      }
+    }
+    double* xp = x0;
+    double* xn = x1;
+    for (int t = 1; t <= Tp; ++t) {
+      const int w = HX - 2 * t, hgt = HY - 2 * t, cnt = w * hgt;
+      for (int it0 = 0; it0 < cnt; it0 += JNT) {
+        int it = it0 + threadIdx.x;
+        double dv = 0.;
+        if (it < cnt) {
+          int lx = it % w + t, ly = it / w + t;
+          int c = ly * HX + lx;
+          // product = (((S x_S + W x_W) + E x_E) + N x_N); the zero centre slot of the
+          // reference CSR row adds an exact zero and is skipped.
+          double p = __dmul_rn(sS[c], xp[c - HX]);
+          p = __dadd_rn(p, __dmul_rn(sW[c], xp[c - 1]));
+          p = __dadd_rn(p, __dmul_rn(sE[c], xp[c + 1]));
+          p = __dadd_rn(p, __dmul_rn(sN[c], xp[c + HX]));
+          double xv = __ddiv_rn(__dsub_rn(sB[c], p), sD[c]);
+          xn[c] = xv;
+          int gi = i0 + lx - TB, gj = j0 + ly - TB;
+          if (lx >= TB && lx < TB + JBX && ly >= TB && ly < TB + JBY && gi < nx && gj < ny)
+            dv = fabs(__dsub_rn(xv, xp[c]));
+        }
+        acc_add(s_acc[t], dv);
+      }
+      __syncthreads();
+      double* tmp = xp;
+      xp = xn;
+      xn = tmp;
+    }
+    for (int it = threadIdx.x; it < JBX * JBY; it += JNT) {
+      int lx = it % JBX + TB, ly = it / JBX + TB;
+      int gi = i0 + lx - TB, gj = j0 + ly - TB;
+      if (gi < nx && gj < ny) xout[(size_t)gj * nx + gi] = xp[ly * HX + lx];
+    }
+    __syncthreads();
+  }
+}
+
+// One CSR pass (one sweep): sparse_matmul (jacobi_iteration.f90:25-43) + update.
+__device__ void csr_pass(const JacobiArgs& a, const double* xin, double* xout, bool first,
+                         unsigned long long (*s_acc)[3]) {
+  const int n = a.nx * a.ny;
+  const int stride = gridDim.x * blockDim.x;
+  for (int base = blockIdx.x * blockDim.x; base < n; base += stride) {
+    int row = base + threadIdx.x;
+    double dv = 0., db = 0.;
+    if (row < n) {
+      double prod = 0.;
+      for (int sp = a.rowstart[row]; sp <= a.rowstart[row + 1] - 1; ++sp)
+        prod = __dadd_rn(prod, __dmul_rn(a.mass[sp - 1], __ldcg(&xin[a.cols[sp - 1] - 1])));
+      double xv = __ddiv_rn(__dsub_rn(a.b[row], prod), a.diag[row]);
+      xout[row] = xv;
+      dv = fabs(__dsub_rn(xv, __ldcg(&xin[row])));
+      db = fabs(0. - a.b[row]);
+    }
+    if (first) acc_add(s_acc[0], db);
+    acc_add(s_acc[1], dv);
+  }
+}
+
+template <int TB, bool CSR>
+__global__ void __launch_bounds__(JNT) jacobi_kernel(const JacobiArgs a) {
+  extern __shared__ __align__(16) double jsm[];
+  __shared__ unsigned long long s_acc[kMaxBlock + 1][3];
+  __shared__ unsigned long long s_tot[kMaxBlock + 1][3];
+  __shared__ int s_ok;
+  JacobiCtl* ctl = a.ctl;
+  int p = *((volatile int*)&ctl->pass_next);
+  const double* xin = a.b;
+  double* xout = a.xa;
+  const double* result = nullptr;
+  bool first = true, zero_result = false, maxhit = false;
+  int k = 0, final_k = 0;
+  const int blk = CSR ? 1 : (a.block < 1 ? 1 : (a.block > TB ? TB : a.block));
+  for (;;) {
+    int Tp = blk;
+    if (a.maxiter - k < Tp) Tp = a.maxiter - k;
+    if (Tp < 1) Tp = 1;
+    for (int q = threadIdx.x; q < (kMaxBlock + 1) * 3; q += blockDim.x) (&s_acc[0][0])[q] = 0ull;
+    __syncthreads();
+    if (CSR)
+      csr_pass(a, xin, xout, first, s_acc);
+    else
+      stencil_pass<TB>(a, xin, xout, Tp, first, s_acc, jsm);
+    __syncthreads();
+    const int slot = p % kResSlots;
+    if (threadIdx.x < (Tp + 1) * 3) {
+      int t = threadIdx.x / 3, l = threadIdx.x % 3;
+      unsigned long long v = s_acc[t][l];
+      if (v) atomicAdd(&ctl->acc[slot][t][l], v);
+    }
+    if (!grid_barrier(ctl, a.spin_limit, &s_ok)) return;
+    if (threadIdx.x < (Tp + 1) * 3) {
+      int t = threadIdx.x / 3, l = threadIdx.x % 3;
+      s_tot[t][l] = __ldcg(&ctl->acc[slot][t][l]);
+    }
+    if (blockIdx.x == 0) {  // recycle the slot of pass p-1 (read by everyone before barrier p)
+      const int z = (p + 2) % kResSlots;
+      for (int q = threadIdx.x; q < (kMaxBlock + 1) * 3; q += blockDim.x)
+        (&ctl->acc[z][0][0])[q] = 0ull;
+      __threadfence();
+    }
+    __syncthreads();
+    p++;
+    int stop = -1;
+    if (first && limbs_le(s_tot[0][0], s_tot[0][1], s_tot[0][2], a.thresh)) {
+      stop = 0;
+    } else {
+      for (int t = 1; t <= Tp; ++t)
+        if (limbs_le(s_tot[t][0], s_tot[t][1], s_tot[t][2], a.thresh)) {
+          stop = t;
+          break;
+        }
+    }
+    first = false;
+    if (stop == 0) {
+      zero_result = true;
+      final_k = 0;
+      break;
+    }
+    if (stop > 0) {
+      final_k = k + stop;
+      if (stop < Tp && !CSR) {  // the stop falls inside the pass: redo it with `stop` sweeps
+        for (int q = threadIdx.x; q < (kMaxBlock + 1) * 3; q += blockDim.x)
+          (&s_acc[0][0])[q] = 0ull;
+        __syncthreads();
+        stencil_pass<TB>(a, xin, xout, stop, false, s_acc, jsm);
+        if (!grid_barrier(ctl, a.spin_limit, &s_ok)) return;
+        if (blockIdx.x == 0) {
+          const int z = (p + 2) % kResSlots;
+          for (int q = threadIdx.x; q < (kMaxBlock + 1) * 3; q += blockDim.x)
+            (&ctl->acc[z][0][0])[q] = 0ull;
+          __threadfence();
+        }
+        p++;
+      }
+      result = xout;
+      break;
+    }
+    k += Tp;
+    if (k >= a.maxiter) {
+      final_k = k;
+      maxhit = true;
+      result = xout;
+      break;
+    }
+    xin = xout;
+    xout = (xout == a.xa) ? a.xb : a.xa;
+  }
+  // deliver the final iterate (haVec of the reference) to its destination
+  const int n = a.nx * a.ny;
+  if (zero_result || result != a.out) {
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x)
+      a.out[q] = zero_result ? 0. : __ldcg(&result[q]);
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    ctl->iters[a.solve_idx] = final_k;
+    if (maxhit && ctl->status == 0) ctl->status = 1;
+    *((volatile int*)&ctl->pass_next) = p;
+  }
+}
+
+template <int TB, bool CSR>
+static const void* jacobi_fn() {
+  return reinterpret_cast<const void*>(&jacobi_kernel<TB, CSR>);
+}
+
+static const void* pick_jacobi(bool csr, int block, size_t* smem) {
+  if (csr) {
+    *smem = 0;
+    return jacobi_fn<1, true>();
+  }
+  if (block <= 1) {
+    *smem = JTile<1>::bytes;
+    return jacobi_fn<1, false>();
+  }
+  if (block <= 2) {
+    *smem = JTile<2>::bytes;
+    return jacobi_fn<2, false>();
+  }
+  if (block <= 4) {
+    *smem = JTile<4>::bytes;
+    return jacobi_fn<4, false>();
+  }
+  *smem = JTile<8>::bytes;
+  return jacobi_fn<8, false>();
+}
+
+int jacobi_grid_blocks(bool csr, int block, int device) {
+  size_t smem = 0;
+  const void* fn = pick_jacobi(csr, block, &smem);
+  if (smem > 48 * 1024)
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, JNT, smem) != cudaSuccess)
+    return -1;
+  int sms = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  if (per_sm < 1) return -1;
+  return per_sm * sms;
+}
+
+cudaError_t launch_jacobi(const JacobiArgs& a, bool csr, int grid_blocks, cudaStream_t s) {
+  size_t smem = 0;
+  const void* fn = pick_jacobi(csr, a.block, &smem);
+  int n = a.nx * a.ny;
+  int blocks = grid_blocks;
+  if (csr) {
+    int need = (n + JNT - 1) / JNT;
+    if (need < blocks) blocks = need;
+  } else {
+    int tiles = ((a.nx + JBX - 1) / JBX) * ((a.ny + JBY - 1) / JBY);
+    if (tiles < blocks) blocks = tiles;
+  }
+  if (blocks < 1) blocks = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(blocks);
+  cfg.blockDim = dim3(JNT);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  void* args[] = {const_cast<JacobiArgs*>(&a)};
+  return cudaLaunchKernelExC(&cfg, fn, args);
+}
+
+}  // namespace swm

@@ -1,0 +1,107 @@
+// swm_kernels.cuh -- declarations shared by the host orchestration and the
+// memory-bound kernels (dt, layouts, Patankar assembly, Jacobi).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "swm_device.cuh"
+#include "swm_rhs.cuh"
+
+namespace swm {
+
+// Residual accumulator: |dx| in units of 2^-100 split into three 40-bit limbs.
+// Integer addition is associative, so the residual sum (and with it the Jacobi
+// stop index) does not depend on tiling, launch shape or atomic ordering.
+constexpr int kResSlots = 3;    // ring of pass slots (see jacobi kernels)
+constexpr int kMaxBlock = 8;    // max Jacobi sweeps per stencil pass
+constexpr int kMaxSolves = 16;  // solves recorded per step
+
+struct JacobiCtl {
+  unsigned long long acc[kResSlots][kMaxBlock + 1][3];  // [slot][0 = initial, 1..T sweeps][limb]
+  unsigned int bar_count;
+  unsigned int bar_gen;
+  int iters[kMaxSolves];  // iterations of each solve of the current step
+  int status;             // 0 ok, 1 maxiter, -4 watchdog
+  int pass_next;          // pass counter carried across solves (slot ring position)
+};
+
+struct AssembleArgs {
+  int nx, ny;
+  double dx, dy;
+  int m;                  // substep 2..4 (1-based, as in the reference)
+  int msteps;             // 4 (mPDeC5) or 2 (mPDeC2)
+  int compat2;            // mPDeC2 sequence-association read of hp
+  double theta[4];        // thetaDeC(m, 1:4)
+  const double* dt;       // device scalar
+  const double* hu_n;     // Ua(1, 2:3) = U^n momentum
+  const double* hv_n;
+  const double* fu[4];    // FUp(r, 2) planes
+  const double* fv[4];    // FUp(r, 3)
+  const double* fxm[4];   // mass fluxes of stage r: [ny][nx+1]
+  const double* fym[4];   // [ny+1][nx]
+  const double* hp[4];    // Up(r, 1) for r = 1..msteps (hp(m,.) is hp[m-1])
+  double* hu_out;         // Ua(m, 2:3)
+  double* hv_out;
+  // stencil layout: 5 planes (S, W, E, N, Diag); CSR layout: mass[5N], diag[N]
+  double* cS;
+  double* cW;
+  double* cE;
+  double* cN;
+  double* cD;
+  double* csr_mass;
+  double* csr_diag;
+  double* rhs_out;        // nullable: rhs = hp(1,.) (needed when hp is read through compat2)
+};
+
+struct JacobiArgs {
+  int nx, ny;
+  int solve_idx;          // slot in ctl->iters
+  int maxiter;
+  unsigned long long thresh[3];  // tol * n in residual units (limbs)
+  const double* b;        // rhs (= hp(1) = h^n)
+  // stencil coefficients
+  const double* cS;
+  const double* cW;
+  const double* cE;
+  const double* cN;
+  const double* cD;
+  // CSR
+  const int* rowstart;    // 1-based (finitevolume.f90:230,267)
+  const int* cols;        // 1-based
+  const double* mass;
+  const double* diag;
+  double* xa;             // ping-pong buffers
+  double* xb;
+  double* out;            // final iterate destination
+  JacobiCtl* ctl;
+  int block;              // sweeps per pass (stencil)
+  long long spin_limit;   // grid-barrier watchdog
+};
+
+struct DtArgs {
+  int nx, ny;
+  double g;
+  const double* h;
+  const double* hu;
+  const double* hv;
+  unsigned long long* lam;  // [2] bit patterns of LambdaMaxX/Y (non-negative doubles)
+  int* bad;                 // non-finite or negative depth seen
+};
+
+// Host launchers (swm_kernels.cu, swm_rhs_*.cu)
+cudaError_t launch_rhs_fast(int mode, const RhsArgs& a, cudaStream_t s);
+cudaError_t launch_rhs_exact(const RhsArgs& a, cudaStream_t s);
+size_t rhs_smem_bytes(int mode);
+
+cudaError_t launch_dt(const DtArgs& a, cudaStream_t s);
+cudaError_t launch_assemble(const AssembleArgs& a, bool csr, cudaStream_t s);
+cudaError_t launch_jacobi(const JacobiArgs& a, bool csr, int grid_blocks, cudaStream_t s);
+int jacobi_grid_blocks(bool csr, int block, int device);
+cudaError_t launch_ghosted_to_planes(const double* G, int nx, int ny, double* h, double* hu,
+                                     double* hv, cudaStream_t s);
+cudaError_t launch_planes_to_ghosted(const double* h, const double* hu, const double* hv, int nx,
+                                     int ny, double* G, double* Vg, cudaStream_t s);
+cudaError_t launch_summary(const double* h, int n, double* out /*[2]*/, cudaStream_t s);
+void residual_limbs_host(double v, unsigned long long out[3]);
+
+}  // namespace swm

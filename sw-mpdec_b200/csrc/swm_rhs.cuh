@@ -1,0 +1,411 @@
+// swm_rhs.cuh -- fused FV right-hand side of one mPDeC stage (sm_100a).
+//
+// One CTA owns a TX x TY tile of cells and performs, in shared memory, everything
+// FVTimeDerivative (finitevolume.f90:402-440) does for those cells:
+//   periodic halo + ConsToPrim   (equation.f90:556-782; halo read with wrapped indices)
+//   WENO5 x: first sweeps along x, second sweeps along y (reconstruction.f90:408-458)
+//   positivity limiter on h     (finitevolume.f90:646-698; seam quirk kept: the
+//                                wrapped cell to the right of the domain is not limited)
+//   Rusanov at 4 Gauss points + Gauss sum (finitevolume.f90:546-590)
+//   the same for y              (reconstruction.f90:464-514, finitevolume.f90:596-757)
+//   bathymetry source           (equation.f90:284-413; depth only, 4x4 interior GPs)
+//   WB subtraction + momentum update + mass face fluxes (finitevolume.f90:446-540)
+// The first sweeps are computed once per (column,row) and shared by the five
+// cells whose stencils use them (the reference recomputes them per cell).
+//
+// Outputs: momentum RHS (Ut(2:3)) and the WB-subtracted mass fluxes FX(1,.), FY(1,.),
+// from which the Patankar production/destruction entries are formed exactly as
+// UpdateTimeDerivative does (finitevolume.f90:500-523); optionally all flux
+// components and the source (WB capture and diagnostics).
+#pragma once
+#include <type_traits>
+
+#include "swm_device.cuh"
+
+namespace swm {
+
+struct RhsArgs {
+  Grid gr;
+  const double* h;
+  const double* hu;
+  const double* hv;     // state planes [ny][nx]
+  double* ut_hu;
+  double* ut_hv;        // momentum RHS [ny][nx]
+  double* fxm;          // mass flux at x faces [ny][nx+1] (face f = left face of cell f)
+  double* fym;          // mass flux at y faces [ny+1][nx]
+  double* fx_full;      // nullable: [3][ny][nx+1]
+  double* fy_full;      // nullable: [3][ny+1][nx]
+  double* s_full;       // nullable: [3][ny][nx]
+  const double* fx_wb;  // nullable: WB reference fluxes, same layouts
+  const double* fy_wb;
+  const double* s_wb;
+  const double* gauss_ex;  // nullable: Gaussian factors exp(-ax (x_q-cx)^2) [nx][4]
+  const double* gauss_ey;  // nullable: exp(-ay (y_q-cy)^2) [ny][4]
+  // nullable: b_x, b_y at the 16 interior Gauss points of every cell, evaluated on the
+  // host with the analytic formula (equation.f90:451-509), planes [4][4][2][ny*nx]
+  const double* bgrad;
+};
+
+constexpr int RHS_TX = 32;
+constexpr int RHS_TY = 8;
+constexpr int RHS_NT = 256;
+
+// Shared-memory plan (element counts).
+template <typename T>
+struct RhsSmem {
+  static constexpr int TX = RHS_TX, TY = RHS_TY;
+  static constexpr int VX = TX + 6, VY = TY + 6;                  // V tile incl. 3-cell halo
+  static constexpr int nV = 3 * VY * VX;                          // double
+  static constexpr int F1X = (TY + 4) * (TX + 2);                 // x first sweeps
+  static constexpr int F1Y = (TY + 2) * (TX + 4);                 // y first sweeps
+  static constexpr int nF1 = 2 * 3 * (F1X > F1Y ? F1X : F1Y);     // T
+  static constexpr int WX = TY * (TX + 2);                        // x face-value cells
+  static constexpr int WY = (TY + 2) * TX;                        // y face-value cells
+  static constexpr int nW = 2 * 3 * 4 * (WX > WY ? WX : WY);      // double
+  static constexpr int nFX = 3 * TY * (TX + 1);                   // double
+  static constexpr int nFY = 3 * (TY + 1) * TX;                   // double
+  static constexpr size_t bytes =
+      sizeof(double) * (nV + nW + nFX + nFY) + sizeof(T) * nF1;
+};
+
+}  // namespace swm
+
+#ifdef SWM_RHS_NS
+// The kernel is compiled in two translation units (EXACT with -fmad=false, FAST
+// with contraction); the namespace keeps their host stubs apart.
+namespace swm {
+namespace SWM_RHS_NS {
+
+// MODE: 0 FP64 (EXACT per translation unit), 1 SPLIT.
+template <int MODE>
+__global__ void __launch_bounds__(RHS_NT, 2) rhs_kernel(const RhsArgs a) {
+  using T = typename std::conditional<MODE == 1, float, double>::type;
+  constexpr bool EX = (MODE == 0) && SWM_EXACT;
+  constexpr int TX = RHS_TX, TY = RHS_TY, NT = RHS_NT;
+  using SM = RhsSmem<T>;
+  constexpr int VX = SM::VX, VY = SM::VY;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* sV = reinterpret_cast<double*>(smem_raw);  // [3][VY][VX]
+  double* sW = sV + SM::nV;                          // [2][3][4][cells]
+  double* sFX = sW + SM::nW;                         // [3][TY][TX+1]
+  double* sFY = sFX + SM::nFX;                       // [3][TY+1][TX]
+  T* sF1 = reinterpret_cast<T*>(sFY + SM::nFY);      // [2][3][...]
+
+  const Grid& gr = a.gr;
+  const int nx = gr.nx, ny = gr.ny;
+  const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
+  const int tid = threadIdx.x;
+
+  // ---- load the haloed tile, V = ConsToPrim(U) (equation.f90:778-782) ----
+  for (int it = tid; it < VY * VX; it += NT) {
+    int cx = it % VX, cy = it / VX;
+    int gi = wrap(i0 - 3 + cx, nx), gj = wrap(j0 - 3 + cy, ny);
+    size_t k = (size_t)gj * nx + gi;
+    double h = a.h[k], hu = a.hu[k], hv = a.hv[k], u, v;
+    cons_to_prim(h, hu, hv, u, v);
+    sV[(0 * VY + cy) * VX + cx] = h;
+    sV[(1 * VY + cy) * VX + cx] = u;
+    sV[(2 * VY + cy) * VX + cx] = v;
+  }
+  __syncthreads();
+#define SV(v, y, x) sV[((v) * VY + (y)) * VX + (x)]
+
+  // ======================= x direction =======================
+  {
+    constexpr int FW = TX + 2, FH = TY + 4;  // first sweeps: cols i0-1..i0+TX, rows j0-2..j0+TY+1
+    T* sTM = sF1;
+    T* sTP = sF1 + 3 * FH * FW;
+    for (int it = tid; it < 3 * FH * FW; it += NT) {
+      int cc = it % FW, rest = it / FW, rr = rest % FH, v = rest / FH;
+      const double* q = &SV(v, rr + 1, cc);  // V cols (i0-1+cc)-2 .. +2 -> tile cols cc..cc+4
+      T wm, wp;
+      if constexpr (MODE == 1) {
+        double c0 = q[2];
+        weno5_first<T, false>((T)(q[0] - c0), (T)(q[1] - c0), T(0), (T)(q[3] - c0),
+                              (T)(q[4] - c0), wm, wp);
+      } else {
+        weno5_first<T, EX>((T)q[0], (T)q[1], (T)q[2], (T)q[3], (T)q[4], wm, wp);
+      }
+      sTM[(v * FH + rr) * FW + cc] = wm;
+      sTP[(v * FH + rr) * FW + cc] = wp;
+    }
+    __syncthreads();
+    // second sweeps along y; cells: cols i0-1..i0+TX (cc), rows j0..j0+TY-1 (rr)
+    constexpr int WC = TY * FW;
+    for (int it = tid; it < 3 * WC; it += NT) {
+      int cc = it % FW, rest = it / FW, rr = rest % TY, v = rest / TY;
+      double wmv[4], wpv[4];
+      const double Vc = SV(v, rr + 3, cc + 2);
+      if constexpr (MODE == 1) {
+        float dm[4], dp[4];
+        T qm[5], qp[5];
+#pragma unroll
+        for (int k = 0; k < 5; ++k) {
+          T base = (T)(SV(v, rr + 1 + k, cc + 2) - Vc);  // row offset to the centre row
+          qm[k] = base + sTM[(v * FH + rr + k) * FW + cc];
+          qp[k] = base + sTP[(v * FH + rr + k) * FW + cc];
+        }
+        weno5_second<T, false>(qm[0], qm[1], qm[2], qm[3], qm[4], dm);
+        weno5_second<T, false>(qp[0], qp[1], qp[2], qp[3], qp[4], dp);
+        const int gc = i0 - 1 + cc;
+        if (v == 0 && gc != nx) {
+          limit_h_dev(gr, Vc, dm, dp, wmv, wpv);
+        } else {
+#pragma unroll
+          for (int g = 0; g < 4; ++g) {
+            wmv[g] = Vc + (double)dm[g];
+            wpv[g] = Vc + (double)dp[g];
+          }
+        }
+      } else {
+        const T* cm = &sTM[(v * FH + rr) * FW + cc];
+        const T* cp = &sTP[(v * FH + rr) * FW + cc];
+        T tm[4], tp[4];
+        weno5_second<T, EX>(cm[0], cm[FW], cm[2 * FW], cm[3 * FW], cm[4 * FW], tm);
+        weno5_second<T, EX>(cp[0], cp[FW], cp[2 * FW], cp[3 * FW], cp[4 * FW], tp);
+#pragma unroll
+        for (int g = 0; g < 4; ++g) {
+          wmv[g] = tm[g];
+          wpv[g] = tp[g];
+        }
+        const int gc = i0 - 1 + cc;
+        if (v == 0 && gc != nx) limit_h(gr, Vc, wmv, wpv);
+      }
+#pragma unroll
+      for (int g = 0; g < 4; ++g) {
+        sW[((0 * 3 + v) * 4 + g) * WC + rr * FW + cc] = wmv[g];
+        sW[((1 * 3 + v) * 4 + g) * WC + rr * FW + cc] = wpv[g];
+      }
+    }
+    __syncthreads();
+    // Rusanov at faces f = i0 .. i0+TX (ff), rows rr; left = WP(cell f-1) (cc = ff), right = WM(f)
+    for (int it = tid; it < TY * (TX + 1); it += NT) {
+      int ff = it % (TX + 1), rr = it / (TX + 1);
+      double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+#pragma unroll
+      for (int g = 0; g < 4; ++g) {
+        const int L = rr * FW + ff, R = rr * FW + ff + 1;
+        double F0, F1, F2;
+        rusanov(gr.g, sW[((1 * 3 + 0) * 4 + g) * WC + L], sW[((1 * 3 + 1) * 4 + g) * WC + L],
+                sW[((1 * 3 + 2) * 4 + g) * WC + L], sW[((0 * 3 + 0) * 4 + g) * WC + R],
+                sW[((0 * 3 + 1) * 4 + g) * WC + R], sW[((0 * 3 + 2) * 4 + g) * WC + R], F0, F1,
+                F2);
+        s0 = s0 + gr.qw[g] * F0;
+        s1 = s1 + gr.qw[g] * F1;
+        s2 = s2 + gr.qw[g] * F2;
+      }
+      sFX[(0 * TY + rr) * (TX + 1) + ff] = s0;
+      sFX[(1 * TY + rr) * (TX + 1) + ff] = s1;
+      sFX[(2 * TY + rr) * (TX + 1) + ff] = s2;
+    }
+    __syncthreads();
+  }
+
+  // ======================= y direction =======================
+  {
+    constexpr int FW = TX + 4, FH = TY + 2;  // first sweeps: cols i0-2..i0+TX+1, rows j0-1..j0+TY
+    T* sTM = sF1;
+    T* sTP = sF1 + 3 * FH * FW;
+    for (int it = tid; it < 3 * FH * FW; it += NT) {
+      int cc = it % FW, rest = it / FW, rr = rest % FH, v = rest / FH;
+      // V rows (j0-1+rr)-2 .. +2 -> tile rows rr..rr+4; col (i0-2+cc) -> tile col cc+1
+      double q0 = SV(v, rr, cc + 1), q1 = SV(v, rr + 1, cc + 1), q2 = SV(v, rr + 2, cc + 1),
+             q3 = SV(v, rr + 3, cc + 1), q4 = SV(v, rr + 4, cc + 1);
+      T wm, wp;
+      if constexpr (MODE == 1) {
+        weno5_first<T, false>((T)(q0 - q2), (T)(q1 - q2), T(0), (T)(q3 - q2), (T)(q4 - q2), wm,
+                              wp);
+      } else {
+        weno5_first<T, EX>((T)q0, (T)q1, (T)q2, (T)q3, (T)q4, wm, wp);
+      }
+      sTM[(v * FH + rr) * FW + cc] = wm;
+      sTP[(v * FH + rr) * FW + cc] = wp;
+    }
+    __syncthreads();
+    // second sweeps along x; cells: cols i0..i0+TX-1 (cc), rows j0-1..j0+TY (rr)
+    constexpr int WC = FH * TX;
+    for (int it = tid; it < 3 * WC; it += NT) {
+      int cc = it % TX, rest = it / TX, rr = rest % FH, v = rest / FH;
+      double wmv[4], wpv[4];
+      const double Vc = SV(v, rr + 2, cc + 3);
+      const int gr_row = j0 - 1 + rr;
+      if constexpr (MODE == 1) {
+        float dm[4], dp[4];
+        T qm[5], qp[5];
+#pragma unroll
+        for (int k = 0; k < 5; ++k) {
+          T base = (T)(SV(v, rr + 2, cc + 1 + k) - Vc);
+          qm[k] = base + sTM[(v * FH + rr) * FW + cc + k];
+          qp[k] = base + sTP[(v * FH + rr) * FW + cc + k];
+        }
+        weno5_second<T, false>(qm[0], qm[1], qm[2], qm[3], qm[4], dm);
+        weno5_second<T, false>(qp[0], qp[1], qp[2], qp[3], qp[4], dp);
+        if (v == 0 && gr_row != ny) {
+          limit_h_dev(gr, Vc, dm, dp, wmv, wpv);
+        } else {
+#pragma unroll
+          for (int g = 0; g < 4; ++g) {
+            wmv[g] = Vc + (double)dm[g];
+            wpv[g] = Vc + (double)dp[g];
+          }
+        }
+      } else {
+        const T* cm = &sTM[(v * FH + rr) * FW + cc];
+        const T* cp = &sTP[(v * FH + rr) * FW + cc];
+        T tm[4], tp[4];
+        weno5_second<T, EX>(cm[0], cm[1], cm[2], cm[3], cm[4], tm);
+        weno5_second<T, EX>(cp[0], cp[1], cp[2], cp[3], cp[4], tp);
+#pragma unroll
+        for (int g = 0; g < 4; ++g) {
+          wmv[g] = tm[g];
+          wpv[g] = tp[g];
+        }
+        if (v == 0 && gr_row != ny) limit_h(gr, Vc, wmv, wpv);
+      }
+#pragma unroll
+      for (int g = 0; g < 4; ++g) {
+        sW[((0 * 3 + v) * 4 + g) * WC + rr * TX + cc] = wmv[g];
+        sW[((1 * 3 + v) * 4 + g) * WC + rr * TX + cc] = wpv[g];
+      }
+    }
+    __syncthreads();
+    // Rusanov at faces f = j0 .. j0+TY (fr); below = WP(row f-1) (rr = fr), above = WM(f)
+    for (int it = tid; it < (TY + 1) * TX; it += NT) {
+      int cc = it % TX, fr = it / TX;
+      double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+#pragma unroll
+      for (int g = 0; g < 4; ++g) {
+        const int L = fr * TX + cc, R = (fr + 1) * TX + cc;
+        double F0, F1, F2;
+        // normal = v (var 2), tangential = u (var 1)
+        rusanov(gr.g, sW[((1 * 3 + 0) * 4 + g) * WC + L], sW[((1 * 3 + 2) * 4 + g) * WC + L],
+                sW[((1 * 3 + 1) * 4 + g) * WC + L], sW[((0 * 3 + 0) * 4 + g) * WC + R],
+                sW[((0 * 3 + 2) * 4 + g) * WC + R], sW[((0 * 3 + 1) * 4 + g) * WC + R], F0, F1,
+                F2);
+        s0 = s0 + gr.qw[g] * F0;
+        s1 = s1 + gr.qw[g] * F2;  // hu component
+        s2 = s2 + gr.qw[g] * F1;  // hv component
+      }
+      sFY[(0 * (TY + 1) + fr) * TX + cc] = s0;
+      sFY[(1 * (TY + 1) + fr) * TX + cc] = s1;
+      sFY[(2 * (TY + 1) + fr) * TX + cc] = s2;
+    }
+    __syncthreads();
+  }
+
+  // ======================= source term (depth only) =======================
+  const bool has_src = gr.bathy > 0;
+  constexpr int SW_ = TX + 4;  // y-sweep columns i0-2..i0+TX+1
+  T* sVt = sF1;                // [4][TY][TX+4]
+  if (has_src) {
+    for (int it = tid; it < TY * SW_; it += NT) {
+      int cc = it % SW_, rr = it / SW_;
+      // U(1) = V(1) = h; rows (j0+rr)-2..+2 -> tile rows rr+1..rr+5; col i0-2+cc -> cc+1
+      double q0 = SV(0, rr + 1, cc + 1), q1 = SV(0, rr + 2, cc + 1), q2 = SV(0, rr + 3, cc + 1),
+             q3 = SV(0, rr + 4, cc + 1), q4 = SV(0, rr + 5, cc + 1);
+      T w[4];
+      if constexpr (MODE == 1)
+        weno5_second<T, false>((T)(q0 - q2), (T)(q1 - q2), T(0), (T)(q3 - q2), (T)(q4 - q2), w);
+      else
+        weno5_second<T, EX>((T)q0, (T)q1, (T)q2, (T)q3, (T)q4, w);
+#pragma unroll
+      for (int g = 0; g < 4; ++g) sVt[(g * TY + rr) * SW_ + cc] = w[g];
+    }
+    __syncthreads();
+  }
+
+  // ======================= per-cell epilogue =======================
+  for (int it = tid; it < TX * TY; it += NT) {
+    int cc = it % TX, rr = it / TX;
+    int gi = i0 + cc, gj = j0 + rr;
+    if (gi >= nx || gj >= ny) continue;
+    double S1 = 0.0, S2 = 0.0;
+    if (has_src) {
+      double hq[4][4];  // [x-GP a][y-GP b]
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        const T* r = &sVt[(b * TY + rr) * SW_ + cc];
+        T w[4];
+        if constexpr (MODE == 1) {
+          const double hc = SV(0, rr + 3, cc + 3);
+          T q[5];
+#pragma unroll
+          for (int k = 0; k < 5; ++k) q[k] = (T)(SV(0, rr + 3, cc + 1 + k) - hc) + r[k];
+          weno5_second<T, false>(q[0], q[1], q[2], q[3], q[4], w);
+#pragma unroll
+          for (int aa = 0; aa < 4; ++aa) hq[aa][b] = hc + (double)w[aa];
+        } else {
+          weno5_second<T, EX>(r[0], r[1], r[2], r[3], r[4], w);
+#pragma unroll
+          for (int aa = 0; aa < 4; ++aa) hq[aa][b] = (double)w[aa];
+        }
+      }
+      // S = sum_{a (x-GP)} sum_{b (y-GP)} W(a,b) * SourceFunc (equation.f90:380-388, :408-410)
+#pragma unroll
+      for (int aa = 0; aa < 4; ++aa) {
+        double X = gp_coord(gr, 0, gi, aa);
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+          double bx, by;
+          if (a.bgrad) {  // host-tabulated analytic gradient, [x-GP][y-GP][comp][cell]
+            const size_t nc = (size_t)nx * ny, cell = (size_t)gj * nx + gi;
+            bx = a.bgrad[((aa * 4 + b) * 2 + 0) * nc + cell];
+            by = a.bgrad[((aa * 4 + b) * 2 + 1) * nc + cell];
+          } else if (gr.bathy == BATHY_GAUSS && a.gauss_ex) {
+            double Y = gp_coord(gr, 1, gj, b);
+            double B = gr.bp[0] * (a.gauss_ex[gi * 4 + aa] * a.gauss_ey[gj * 4 + b]);
+            bx = (-2.0 * gr.bp[1] * (X - gr.bp[2])) * B;
+            by = (-2.0 * gr.bp[3] * (Y - gr.bp[4])) * B;
+          } else {
+            bathy_grad(gr, X, gp_coord(gr, 1, gj, b), bx, by);
+          }
+          double gh = gr.g * hq[aa][b];
+          S1 = S1 + gr.wgp[aa][b] * (-(gh * bx));
+          S2 = S2 + gr.wgp[aa][b] * (-(gh * by));
+        }
+      }
+    }
+    double fxl[3], fxr[3], fyb[3], fyt[3], s[3] = {0.0, S1, S2};
+#pragma unroll
+    for (int v = 0; v < 3; ++v) {
+      fxl[v] = sFX[(v * TY + rr) * (TX + 1) + cc];
+      fxr[v] = sFX[(v * TY + rr) * (TX + 1) + cc + 1];
+      fyb[v] = sFY[(v * (TY + 1) + rr) * TX + cc];
+      fyt[v] = sFY[(v * (TY + 1) + rr + 1) * TX + cc];
+    }
+    const size_t kx = (size_t)gj * (nx + 1) + gi, ky = (size_t)gj * nx + gi, kc = ky;
+    const size_t sfx = (size_t)ny * (nx + 1), sfy = (size_t)(ny + 1) * nx, sc = (size_t)nx * ny;
+    if (a.fx_wb) {  // FX = FX - FXWB etc. (finitevolume.f90:485-489)
+#pragma unroll
+      for (int v = 0; v < 3; ++v) {
+        fxl[v] = fxl[v] - a.fx_wb[v * sfx + kx];
+        fxr[v] = fxr[v] - a.fx_wb[v * sfx + kx + 1];
+        fyb[v] = fyb[v] - a.fy_wb[v * sfy + ky];
+        fyt[v] = fyt[v] - a.fy_wb[v * sfy + ky + nx];
+        s[v] = s[v] - a.s_wb[v * sc + kc];
+      }
+    }
+    // Ut(2:3) = S - (FX(i)-FX(i-1))/dx - (FY(j)-FY(j-1))/dy (finitevolume.f90:525-527)
+    a.ut_hu[kc] = s[1] - (fxr[1] - fxl[1]) / gr.dx - (fyt[1] - fyb[1]) / gr.dy;
+    a.ut_hv[kc] = s[2] - (fxr[2] - fxl[2]) / gr.dx - (fyt[2] - fyb[2]) / gr.dy;
+    a.fxm[kx] = fxl[0];
+    a.fym[ky] = fyb[0];
+    if (gi == nx - 1) a.fxm[kx + 1] = fxr[0];
+    if (gj == ny - 1) a.fym[ky + nx] = fyt[0];
+    if (a.fx_full) {
+#pragma unroll
+      for (int v = 0; v < 3; ++v) {
+        a.fx_full[v * sfx + kx] = fxl[v];
+        a.fy_full[v * sfy + ky] = fyb[v];
+        a.s_full[v * sc + kc] = s[v];
+        if (gi == nx - 1) a.fx_full[v * sfx + kx + 1] = fxr[v];
+        if (gj == ny - 1) a.fy_full[v * sfy + ky + nx] = fyt[v];
+      }
+    }
+  }
+#undef SV
+}
+
+}  // namespace SWM_RHS_NS
+}  // namespace swm
+#endif  // SWM_RHS_NS

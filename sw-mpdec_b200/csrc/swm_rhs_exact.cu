@@ -1,0 +1,24 @@
+// swm_rhs_exact.cu -- RHS kernel instance for the EXACT FP64 form.  Built with
+// -fmad=false so that every expression rounds as the reference's source order
+// does; with IEEE division and square root this reproduces the CPU restatement
+// bit for bit except where a libm function (exp, sin, cos) is evaluated.
+#define SWM_EXACT 1
+#define SWM_RHS_NS rhs_exact
+#include "swm_kernels.cuh"
+
+namespace swm {
+
+cudaError_t launch_rhs_exact(const RhsArgs& a, cudaStream_t s) {
+  dim3 grd((a.gr.nx + RHS_TX - 1) / RHS_TX, (a.gr.ny + RHS_TY - 1) / RHS_TY);
+  size_t sm = RhsSmem<double>::bytes;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(rhs_exact::rhs_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)sm);
+    attr = true;
+  }
+  rhs_exact::rhs_kernel<0><<<grd, RHS_NT, sm, s>>>(a);
+  return cudaGetLastError();
+}
+
+}  // namespace swm

@@ -1,0 +1,37 @@
+// swm_rhs_fast.cu -- RHS kernel instances for the FP64 form (FMA contraction,
+// shared reciprocals) and the split FP32/FP64 form.
+#define SWM_EXACT 0
+#define SWM_RHS_NS rhs_fast
+#include "swm_kernels.cuh"
+
+namespace swm {
+
+size_t rhs_smem_bytes(int mode) {
+  return mode == 1 ? RhsSmem<float>::bytes : RhsSmem<double>::bytes;
+}
+
+cudaError_t launch_rhs_fast(int mode, const RhsArgs& a, cudaStream_t s) {
+  dim3 grd((a.gr.nx + RHS_TX - 1) / RHS_TX, (a.gr.ny + RHS_TY - 1) / RHS_TY);
+  if (mode == 1) {
+    size_t sm = RhsSmem<float>::bytes;
+    static bool attr = false;
+    if (!attr) {
+      cudaFuncSetAttribute(rhs_fast::rhs_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)sm);
+      attr = true;
+    }
+    rhs_fast::rhs_kernel<1><<<grd, RHS_NT, sm, s>>>(a);
+  } else {
+    size_t sm = RhsSmem<double>::bytes;
+    static bool attr = false;
+    if (!attr) {
+      cudaFuncSetAttribute(rhs_fast::rhs_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)sm);
+      attr = true;
+    }
+    rhs_fast::rhs_kernel<0><<<grd, RHS_NT, sm, s>>>(a);
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace swm
