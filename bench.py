@@ -252,6 +252,8 @@ def main():
     # accuracy of the split form against the FP64 form on the same steps
     a, b = results["split"]["final"], results["fp64"]["final"]
     l1 = [float(np.abs(a[v] - b[v]).sum() / max(np.abs(b[v]).sum(), 1e-300)) for v in range(3)]
+    area = (c["x1"][0] - c["x0"][0]) * (c["x1"][1] - c["x0"][1]) / cells
+    l1_abs = [float(np.abs(a[v] - b[v]).sum() * area) for v in range(3)]
     hmin = float(a[0].min())
 
     # end to end through the C ABI with host buffers
@@ -300,13 +302,15 @@ def main():
                "jacobi": (pr["jacobi_ms"], pr["jacobi_launches"])}
     dom = max(classes, key=lambda k: classes[k][0])
     prof_iters = sum(results["split"]["prof"].get("iters", []) or []) or nj
-    # algorithmic bytes per launch (per-cell figures of the byte model)
+    # algorithmic bytes per launch: Jacobi 64 B/cell/iteration (5 coefficients, rhs,
+    # x read, x written); RHS 56 B/cell (U read, momentum RHS and the two mass face
+    # fluxes written); combination + assembly 208 B/cell
     if dom == "jacobi":
         alg = 64.0 * cells * prof_iters / max(classes[dom][1], 1)
     elif dom == "rhs":
-        alg = 40.0 * cells
+        alg = 56.0 * cells
     else:
-        alg = 80.0 * cells
+        alg = 208.0 * cells
     t_launch = classes[dom][0] / max(classes[dom][1], 1) * 1e-3
     achieved = alg / t_launch / 1e9
     launches = sum(v[1] for v in classes.values()) + 1  # + dt reduction
@@ -322,7 +326,8 @@ def main():
         "fp64": {"value": value64, "ms_per_step": fp["ms"] / args.steps,
                  "jacobi_iters_per_step": fp["iters"] / args.steps},
         "split_over_fp64": value / value64,
-        "accuracy": {"rel_l1_split_vs_fp64_per_var": l1, "min_h": hmin,
+        "accuracy": {"rel_l1_split_vs_fp64_per_var": l1, "l1_split_vs_fp64_per_var": l1_abs,
+                     "min_h": hmin,
                      "steps": args.steps + args.warmup},
         "jacobi_iters_per_step": nj,
         "kernel_ms_per_step": {k: v[0] for k, v in classes.items()},

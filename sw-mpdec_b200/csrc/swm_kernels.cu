@@ -245,35 +245,36 @@ __global__ void assemble_kernel(const AssembleArgs a, bool csr) {
   const int nj[4] = {wrap(j - 1, ny), j, j, wrap(j + 1, ny)};
   double M[4] = {0., 0., 0., 0.};
   double D = 1.;
+  // For a face flux f only one of P = max(f,0)/len and Q = -min(f,0)/len is non-zero,
+  // and PATANKAR_DIV of a zero entry is a zero that leaves Mass/Diagonal unchanged, so
+  // only the non-zero entry is formed; the non-zero updates keep the reference's order.
 #pragma unroll
   for (int nb = 0; nb < 4; ++nb) {
     const double hL = hp_read(a, m, ni[nb], nj[nb]);
+    const double len = (nb == 0 || nb == 3) ? a.dy : a.dx;
     for (int r = 0; r < ms; ++r) {
-      double f, P, Q;
-      if (nb == 0) {
+      double f;
+      if (nb == 0)
         f = a.fym[r][(size_t)j * nx + i];
-        P = dmax(f, 0.) / a.dy;
-        Q = -dmin(f, 0.) / a.dy;
-      } else if (nb == 1) {
+      else if (nb == 1)
         f = a.fxm[r][(size_t)j * (nx + 1) + i];
-        P = dmax(f, 0.) / a.dx;
-        Q = -dmin(f, 0.) / a.dx;
-      } else if (nb == 2) {
+      else if (nb == 2)
         f = -a.fxm[r][(size_t)j * (nx + 1) + i + 1];
-        P = dmax(f, 0.) / a.dx;
-        Q = -dmin(f, 0.) / a.dx;
-      } else {
+      else
         f = -a.fym[r][(size_t)(j + 1) * nx + i];
-        P = dmax(f, 0.) / a.dy;
-        Q = -dmin(f, 0.) / a.dy;
-      }
       const double th = a.theta[r];
-      if (th > 0.) {
-        M[nb] = M[nb] - dt * th * (patankar_div(P, hL));
-        D = D + dt * th * (patankar_div(Q, hK));
-      } else {
-        D = D - dt * th * (patankar_div(P, hK));
-        M[nb] = M[nb] + dt * th * (patankar_div(Q, hL));
+      if (f > 0.) {  // production P_KL = f/len
+        const double P = f / len;
+        if (th > 0.)
+          M[nb] = M[nb] - dt * th * (patankar_div(P, hL));
+        else
+          D = D - dt * th * (patankar_div(P, hK));
+      } else if (f < 0.) {  // destruction D_KL = -f/len
+        const double Q = -f / len;
+        if (th > 0.)
+          D = D + dt * th * (patankar_div(Q, hK));
+        else
+          M[nb] = M[nb] + dt * th * (patankar_div(Q, hL));
       }
     }
   }
@@ -340,7 +341,7 @@ __device__ bool grid_barrier(JacobiCtl* ctl, long long spin_limit, int* s_ok) {
 }
 
 // Stencil tile geometry
-constexpr int JBX = 64, JBY = 16, JNT = 512;
+constexpr int JBX = 64, JBY = 16, JNT = 256;
 
 template <int TB>
 struct JTile {
@@ -348,25 +349,45 @@ struct JTile {
   static constexpr size_t bytes = sizeof(double) * 8 * HN;
 };
 
-__device__ __forceinline__ void acc_add(unsigned long long* s_acc_t, double v) {
-  unsigned long long l2, l1, l0;
-  residual_limbs(v, l2, l1, l0);
-  l2 = warp_sum_u64(l2);
-  l1 = warp_sum_u64(l1);
-  l0 = warp_sum_u64(l0);
-  if ((threadIdx.x & 31) == 0) {
-    if (l2) atomicAdd(&s_acc_t[0], l2);
-    if (l1) atomicAdd(&s_acc_t[1], l1);
-    if (l0) atomicAdd(&s_acc_t[2], l0);
-  }
+// 16-byte asynchronous global->shared copy through L2 (cp.async.cg); the x iterate
+// of the previous pass was written by other CTAs, so it must not come from L1.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::);
 }
 
-// One stencil pass of Tp <= TB sweeps over every tile of this CTA.
+// Per-thread residual limbs for sweep 0 (initial residual) and sweeps 1..kMaxBlock.
+struct Acc {
+  unsigned long long v[kMaxBlock + 1][3];
+};
+
+__device__ __forceinline__ void acc_put(unsigned long long* a3, double v) {
+  unsigned long long l2, l1, l0;
+  residual_limbs(v, l2, l1, l0);
+  a3[0] += l2;
+  a3[1] += l1;
+  a3[2] += l0;
+}
+
+// periodic index for -n <= g < 2n
+__device__ __forceinline__ int wrap_near(int g, int n) {
+  if (g < 0) g += n;
+  if (g >= n) g -= n;
+  return g;
+}
+
+// One stencil pass of Tp <= TB sweeps over every tile of this CTA.  A tile is a
+// JBX x JBY block of cells plus a TB-cell halo in shared memory; sweep t updates
+// the region shrunk by t, so after Tp sweeps the tile interior holds x^{k+Tp},
+// bit-identical to Tp global sweeps.  Warps own rows, lanes own columns.
 template <int TB>
 __device__ void stencil_pass(const JacobiArgs& a, const double* xin, double* xout, int Tp,
-                             bool first, unsigned long long (*s_acc)[3], double* sm) {
+                             bool first, Acc& acc, double* sm) {
   using G = JTile<TB>;
-  constexpr int HX = G::HX, HY = G::HY, HN = G::HN;
+  constexpr int HX = G::HX, HY = G::HY, HN = G::HN, NW = JNT / 32;
   double* sS = sm;
   double* sW = sS + HN;
   double* sE = sW + HN;
@@ -376,64 +397,92 @@ __device__ void stencil_pass(const JacobiArgs& a, const double* xin, double* xou
   double* x0 = sB + HN;
   double* x1 = x0 + HN;
   const int nx = a.nx, ny = a.ny;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const bool small = (nx < HX) || (ny < HY);
+  // 16-byte pairs need an even first column (i0 - TB) and an even row pitch
+  const bool pairs = (TB % 2 == 0) && !small && (nx % 2 == 0);
   const int tx = (nx + JBX - 1) / JBX, ty = (ny + JBY - 1) / JBY;
   for (int tile = blockIdx.x; tile < tx * ty; tile += gridDim.x) {
     const int i0 = (tile % tx) * JBX, j0 = (tile / tx) * JBY;
-    for (int it = threadIdx.x; it < HN; it += JNT) {
-      int lx = it % HX, ly = it / HX;
-      int gi = wrap(i0 - TB + lx, nx), gj = wrap(j0 - TB + ly, ny);
-      size_t g = (size_t)gj * nx + gi;
-      sS[it] = a.cS[g];
-      sW[it] = a.cW[g];
-      sE[it] = a.cE[g];
-      sN[it] = a.cN[g];
-      sD[it] = a.cD[g];
-      sB[it] = a.b[g];
-      x0[it] = __ldcg(&xin[g]);
+    if (pairs) {
+      // even nx, no multiple wrap: 16-byte pairs (gi even) never straddle the seam
+      for (int ly = warp; ly < HY; ly += NW) {
+        const int gj = wrap_near(j0 - TB + ly, ny);
+        const size_t row = (size_t)gj * nx;
+        for (int lp = lane; lp < HX / 2; lp += 32) {
+          const int lx = 2 * lp;
+          const size_t g = row + wrap_near(i0 - TB + lx, nx);
+          const int c = ly * HX + lx;
+          cp_async16(&sS[c], &a.cS[g]);
+          cp_async16(&sW[c], &a.cW[g]);
+          cp_async16(&sE[c], &a.cE[g]);
+          cp_async16(&sN[c], &a.cN[g]);
+          cp_async16(&sD[c], &a.cD[g]);
+          cp_async16(&sB[c], &a.b[g]);
+          cp_async16(&x0[c], &xin[g]);
+        }
+      }
+      cp_async_wait_all();
+    } else {
+      for (int ly = warp; ly < HY; ly += NW) {
+        int gj = j0 - TB + ly;
+        gj = small ? wrap(gj, ny) : wrap_near(gj, ny);
+        const size_t row = (size_t)gj * nx;
+        for (int lx = lane; lx < HX; lx += 32) {
+          int gi = i0 - TB + lx;
+          gi = small ? wrap(gi, nx) : wrap_near(gi, nx);
+          const size_t g = row + gi;
+          const int c = ly * HX + lx;
+          sS[c] = a.cS[g];
+          sW[c] = a.cW[g];
+          sE[c] = a.cE[g];
+          sN[c] = a.cN[g];
+          sD[c] = a.cD[g];
+          sB[c] = a.b[g];
+          x0[c] = __ldcg(&xin[g]);
+        }
+      }
     }
     __syncthreads();
     if (first) {  // initial residual mean|0 - b| (jacobi_iteration.f90:69)
-      static_assert((JBX * JBY) % JNT == 0, "uniform trip count for the warp reductions");
-      for (int it = threadIdx.x; it < JBX * JBY; it += JNT) {
-        int lx = it % JBX + TB, ly = it / JBX + TB;
-        int gi = i0 + lx - TB, gj = j0 + ly - TB;
-        double v = (gi < nx && gj < ny) ? fabs(0. - sB[ly * HX + lx]) : 0.;
-        acc_add(s_acc[0], v);
-      }
+      for (int ly = TB + warp; ly < TB + JBY; ly += NW)
+        for (int lx = TB + lane; lx < TB + JBX; lx += 32)
+          if (i0 + lx - TB < nx && j0 + ly - TB < ny) acc_put(acc.v[0], fabs(0. - sB[ly * HX + lx]));
     }
     double* xp = x0;
     double* xn = x1;
-    for (int t = 1; t <= Tp; ++t) {
-      const int w = HX - 2 * t, hgt = HY - 2 * t, cnt = w * hgt;
-      for (int it0 = 0; it0 < cnt; it0 += JNT) {
-        int it = it0 + threadIdx.x;
-        double dv = 0.;
-        if (it < cnt) {
-          int lx = it % w + t, ly = it / w + t;
-          int c = ly * HX + lx;
-          // product = (((S x_S + W x_W) + E x_E) + N x_N); the zero centre slot of the
-          // reference CSR row adds an exact zero and is skipped.
-          double p = __dmul_rn(sS[c], xp[c - HX]);
-          p = __dadd_rn(p, __dmul_rn(sW[c], xp[c - 1]));
-          p = __dadd_rn(p, __dmul_rn(sE[c], xp[c + 1]));
-          p = __dadd_rn(p, __dmul_rn(sN[c], xp[c + HX]));
-          double xv = __ddiv_rn(__dsub_rn(sB[c], p), sD[c]);
-          xn[c] = xv;
-          int gi = i0 + lx - TB, gj = j0 + ly - TB;
-          if (lx >= TB && lx < TB + JBX && ly >= TB && ly < TB + JBY && gi < nx && gj < ny)
-            dv = fabs(__dsub_rn(xv, xp[c]));
+#pragma unroll
+    for (int t = 1; t <= TB; ++t) {
+      if (t <= Tp) {
+        for (int ly = t + warp; ly < HY - t; ly += NW) {
+          const bool row_in = ly >= TB && ly < TB + JBY && j0 + ly - TB < ny;
+          for (int lx = t + lane; lx < HX - t; lx += 32) {
+            const int c = ly * HX + lx;
+            // product = (((S x_S + W x_W) + E x_E) + N x_N); the zero centre slot of the
+            // reference CSR row adds an exact zero and is skipped.
+            double p = __dmul_rn(sS[c], xp[c - HX]);
+            p = __dadd_rn(p, __dmul_rn(sW[c], xp[c - 1]));
+            p = __dadd_rn(p, __dmul_rn(sE[c], xp[c + 1]));
+            p = __dadd_rn(p, __dmul_rn(sN[c], xp[c + HX]));
+            const double xv = __ddiv_rn(__dsub_rn(sB[c], p), sD[c]);
+            xn[c] = xv;
+            if (row_in && lx >= TB && lx < TB + JBX && i0 + lx - TB < nx)
+              acc_put(acc.v[t], fabs(__dsub_rn(xv, xp[c])));
+          }
         }
-        acc_add(s_acc[t], dv);
+        __syncthreads();
+        double* tmp = xp;
+        xp = xn;
+        xn = tmp;
       }
-      __syncthreads();
-      double* tmp = xp;
-      xp = xn;
-      xn = tmp;
     }
-    for (int it = threadIdx.x; it < JBX * JBY; it += JNT) {
-      int lx = it % JBX + TB, ly = it / JBX + TB;
-      int gi = i0 + lx - TB, gj = j0 + ly - TB;
-      if (gi < nx && gj < ny) xout[(size_t)gj * nx + gi] = xp[ly * HX + lx];
+    for (int ly = TB + warp; ly < TB + JBY; ly += NW) {
+      const int gj = j0 + ly - TB;
+      if (gj >= ny) continue;
+      for (int lx = TB + lane; lx < TB + JBX; lx += 32) {
+        const int gi = i0 + lx - TB;
+        if (gi < nx) xout[(size_t)gj * nx + gi] = xp[ly * HX + lx];
+      }
     }
     __syncthreads();
   }
@@ -441,28 +490,34 @@ __device__ void stencil_pass(const JacobiArgs& a, const double* xin, double* xou
 
 // One CSR pass (one sweep): sparse_matmul (jacobi_iteration.f90:25-43) + update.
 __device__ void csr_pass(const JacobiArgs& a, const double* xin, double* xout, bool first,
-                         unsigned long long (*s_acc)[3]) {
+                         Acc& acc) {
   const int n = a.nx * a.ny;
-  const int stride = gridDim.x * blockDim.x;
-  for (int base = blockIdx.x * blockDim.x; base < n; base += stride) {
-    int row = base + threadIdx.x;
-    double dv = 0., db = 0.;
-    if (row < n) {
-      double prod = 0.;
-      for (int sp = a.rowstart[row]; sp <= a.rowstart[row + 1] - 1; ++sp)
-        prod = __dadd_rn(prod, __dmul_rn(a.mass[sp - 1], __ldcg(&xin[a.cols[sp - 1] - 1])));
-      double xv = __ddiv_rn(__dsub_rn(a.b[row], prod), a.diag[row]);
-      xout[row] = xv;
-      dv = fabs(__dsub_rn(xv, __ldcg(&xin[row])));
-      db = fabs(0. - a.b[row]);
-    }
-    if (first) acc_add(s_acc[0], db);
-    acc_add(s_acc[1], dv);
+  for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < n; row += gridDim.x * blockDim.x) {
+    double prod = 0.;
+    for (int sp = a.rowstart[row]; sp <= a.rowstart[row + 1] - 1; ++sp)
+      prod = __dadd_rn(prod, __dmul_rn(a.mass[sp - 1], __ldcg(&xin[a.cols[sp - 1] - 1])));
+    const double xv = __ddiv_rn(__dsub_rn(a.b[row], prod), a.diag[row]);
+    xout[row] = xv;
+    acc_put(acc.v[1], fabs(__dsub_rn(xv, __ldcg(&xin[row]))));
+    if (first) acc_put(acc.v[0], fabs(0. - a.b[row]));
   }
 }
 
+// Block reduction of the per-thread limbs into s_acc (sweeps 0..TB).
+template <int TB>
+__device__ __forceinline__ void acc_reduce(Acc& acc, unsigned long long (*s_acc)[3]) {
+#pragma unroll
+  for (int t = 0; t <= TB; ++t)
+#pragma unroll
+    for (int l = 0; l < 3; ++l) {
+      unsigned long long v = warp_sum_u64(acc.v[t][l]);
+      acc.v[t][l] = 0ull;
+      if ((threadIdx.x & 31) == 0 && v) atomicAdd(&s_acc[t][l], v);
+    }
+}
+
 template <int TB, bool CSR>
-__global__ void __launch_bounds__(JNT) jacobi_kernel(const JacobiArgs a) {
+__global__ void __launch_bounds__(JNT, 2) jacobi_kernel(const JacobiArgs a) {
   extern __shared__ __align__(16) double jsm[];
   __shared__ unsigned long long s_acc[kMaxBlock + 1][3];
   __shared__ unsigned long long s_tot[kMaxBlock + 1][3];
@@ -475,6 +530,11 @@ __global__ void __launch_bounds__(JNT) jacobi_kernel(const JacobiArgs a) {
   bool first = true, zero_result = false, maxhit = false;
   int k = 0, final_k = 0;
   const int blk = CSR ? 1 : (a.block < 1 ? 1 : (a.block > TB ? TB : a.block));
+  Acc acc;
+#pragma unroll
+  for (int t = 0; t <= kMaxBlock; ++t)
+#pragma unroll
+    for (int l = 0; l < 3; ++l) acc.v[t][l] = 0ull;
   for (;;) {
     int Tp = blk;
     if (a.maxiter - k < Tp) Tp = a.maxiter - k;
@@ -482,9 +542,10 @@ __global__ void __launch_bounds__(JNT) jacobi_kernel(const JacobiArgs a) {
     for (int q = threadIdx.x; q < (kMaxBlock + 1) * 3; q += blockDim.x) (&s_acc[0][0])[q] = 0ull;
     __syncthreads();
     if (CSR)
-      csr_pass(a, xin, xout, first, s_acc);
+      csr_pass(a, xin, xout, first, acc);
     else
-      stencil_pass<TB>(a, xin, xout, Tp, first, s_acc, jsm);
+      stencil_pass<TB>(a, xin, xout, Tp, first, acc, jsm);
+    acc_reduce<TB>(acc, s_acc);
     __syncthreads();
     const int slot = p % kResSlots;
     if (threadIdx.x < (Tp + 1) * 3) {
@@ -527,7 +588,8 @@ __global__ void __launch_bounds__(JNT) jacobi_kernel(const JacobiArgs a) {
         for (int q = threadIdx.x; q < (kMaxBlock + 1) * 3; q += blockDim.x)
           (&s_acc[0][0])[q] = 0ull;
         __syncthreads();
-        stencil_pass<TB>(a, xin, xout, stop, false, s_acc, jsm);
+        stencil_pass<TB>(a, xin, xout, stop, false, acc, jsm);
+        acc_reduce<TB>(acc, s_acc);
         if (!grid_barrier(ctl, a.spin_limit, &s_ok)) return;
         if (blockIdx.x == 0) {
           const int z = (p + 2) % kResSlots;
