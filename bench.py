@@ -223,12 +223,10 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
+    import replicas
+
     def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return replicas.aggregate(x, 0.0, dist, device="cuda")[0]
 
     results = {}
     clocks = None
