@@ -159,6 +159,29 @@ SWM_API int swm_debug_rhs(swm_handle h, const double *U_ghosted, double *Ut, dou
 SWM_API int swm_debug_jacobi(swm_handle h, const double *mass, const double *diag, const double *rhs,
                      double *sol, int *iters);
 
+/* ---- allocation-free Jacobi solve ----
+ * No counterpart in the reference (its jacobi() works on module arrays).  For
+ * callers that cannot let a library allocate device memory -- drivers that own
+ * every byte through their own pool or share a hard memory cap between solvers,
+ * and loops that must not pay the device-wide synchronisation of cudaMalloc and
+ * cudaFree.  Solves one Patankar system (x <- (rhs - S x_S - W x_W - E x_E - N x_N)/D
+ * on the periodic nx*ny grid, stop rule of jacobi_iteration.f90:52-87) with the
+ * matrix-free stencil kernel, `block` sweeps per pass (1..8).  All arrays are the
+ * caller's device memory, nx*ny doubles each, [ny][nx] row-major; rhs and sol
+ * must not overlap.  Scratch is a static device array sized for at most
+ * 1,048,576 cells (8 MiB plus a small control block), held on every GPU that
+ * loads the library until the process exits; larger grids are rejected with
+ * SWM_ERR_PARAM.  The first call on each device looks up that array's device
+ * address (cudaGetSymbolAddress) and the kernel's resident grid; make that first
+ * call before any stream capture.  Every call shares the scratch: calls whose
+ * work overlaps on the GPU (other streams, other host threads) race.  Runs on
+ * `stream` (a cudaStream_t, 0 = legacy default) and returns after the solve with
+ * the iteration count in *iters. */
+SWM_API int swm_jacobi_noalloc(int nx, int ny, const double *cS, const double *cW,
+                               const double *cE, const double *cN, const double *cD,
+                               const double *rhs, double *sol, int maxiter, double tol,
+                               int block, int *iters, void *stream);
+
 /* ---- batched ensembles ---- */
 typedef struct swm_batch *swm_batch_handle;
 /* n problems of independent size and parameters, stepped together: one

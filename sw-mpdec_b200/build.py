@@ -26,6 +26,7 @@ UNITS = [
     ("swm_rhs_fast.cu", []),
     ("swm_capi.cu", ["-Xcompiler", "-ffp-contract=off"]),
     ("swm_batch.cu", []),
+    ("swm_noalloc.cu", []),
 ]
 
 

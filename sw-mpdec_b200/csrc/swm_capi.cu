@@ -44,6 +44,11 @@ const double kTheta2[2][2] = {{0.0, 0.0}, {0.5, 0.5}};
 
 }  // namespace
 
+namespace swm {
+// Lets other translation units report through swm_last_error().
+void set_last_error(const char* msg) { g_last_error = msg; }
+}  // namespace swm
+
 struct swm_solver {
   swm_params p{};
   int nx = 0, ny = 0;

@@ -27,6 +27,7 @@ EXPORTS = [
     "swm_run", "swm_get_stats", "swm_state_summary", "swm_last_error", "swm_strerror",
     "swm_get_stream", "swm_profile_step", "swm_debug_rhs", "swm_debug_jacobi", "swm_batch_create", "swm_batch_destroy",
     "swm_batch_set_planes", "swm_batch_get_planes", "swm_batch_step", "swm_batch_cells",
+    "swm_jacobi_noalloc",
 ]
 
 
@@ -101,6 +102,9 @@ def load():
     lib.swm_batch_get_planes.argtypes = [vp, ctypes.c_int, dp]
     lib.swm_batch_step.argtypes = [vp, dp]
     lib.swm_batch_cells.argtypes = [vp, P(ctypes.c_longlong)]
+    lib.swm_jacobi_noalloc.argtypes = ([ctypes.c_int, ctypes.c_int] + [vp] * 7 +
+                                       [ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                        P(ctypes.c_int), vp])
     _lib = lib
     return lib
 
@@ -245,6 +249,18 @@ class Solver:
         rc = _check(self.lib.swm_debug_jacobi(self.h, _dp(mass), _dp(diag), _dp(rhs), _dp(sol),
                                               ctypes.byref(it)))
         return sol, it.value, rc
+
+
+def jacobi_noalloc(nx, ny, cS, cW, cE, cN, cD, rhs, sol, maxiter=1000, tol=1e-16, block=4,
+                   stream=0):
+    """swm_jacobi_noalloc: one Patankar Jacobi solve on caller-owned device arrays
+    (integer device addresses), with no allocation by the library.  Returns
+    (iterations, status)."""
+    it = ctypes.c_int()
+    ptrs = [ctypes.c_void_p(int(p)) for p in (cS, cW, cE, cN, cD, rhs, sol)]
+    rc = _check(load().swm_jacobi_noalloc(nx, ny, *ptrs, maxiter, tol, block, ctypes.byref(it),
+                                          ctypes.c_void_p(int(stream))))
+    return it.value, rc
 
 
 class Batch:

@@ -1,0 +1,59 @@
+"""swm_jacobi_noalloc: the Jacobi solve for callers that cannot let a library
+allocate device memory (drivers that own all device memory through their own
+pool or a shared memory cap, loops that cannot afford cudaMalloc/cudaFree's
+device-wide synchronisation).  It must give the same answer as the handle
+solver (swm_debug_jacobi with the stencil solver) on repeated calls, while its
+only scratch is a static device array that keeps the previous call's contents.
+
+This file is named to be collected last."""
+import ctypes
+
+import numpy as np
+import pytest
+
+import swm
+
+
+def patankar_system(n_cells, seed):
+    """An M-matrix in the reference CSR slot order (S, W, C, E, N), positive rhs."""
+    rng = np.random.default_rng(seed)
+    mass = -0.1 * rng.random((n_cells, 5))
+    mass[:, 2] = 0.0
+    diag = 1.0 + 0.4 * rng.random(n_cells)
+    rhs = 0.5 + rng.random(n_cells)
+    return mass, diag, rhs
+
+
+def test_noalloc_rejects_grids_beyond_its_scratch():
+    # size check happens before any CUDA call
+    lib = swm.load()
+    it = ctypes.c_int()
+    one = ctypes.c_void_p(16)
+    rc = lib.swm_jacobi_noalloc(2048, 2048, *([one] * 6), ctypes.c_void_p(32), 1000, 1e-16, 4,
+                                ctypes.byref(it), None)
+    assert rc == -1
+    assert b"1048576" in lib.swm_last_error()
+
+
+@pytest.mark.gpu
+def test_noalloc_matches_handle_solver_twice(gpu):
+    import torch
+    nx, ny, block = 96, 80, 4
+    N = nx * ny
+    s = swm.Solver(nx=nx, ny=ny, x0=(0.0, 0.0), x1=(1.0, 1.0), solver="stencil",
+                   jacobi_block=block)
+    dev = torch.device("cuda", 0)
+    for call, seed in enumerate((11, 12)):
+        mass, diag, rhs = patankar_system(N, seed)
+        ref, k_ref, rc_ref = s.debug_jacobi(mass.reshape(-1), diag, rhs)
+        planes = [torch.from_numpy(np.ascontiguousarray(mass[:, k])).to(dev)
+                  for k in (0, 1, 3, 4)]
+        cD = torch.from_numpy(diag).to(dev)
+        b = torch.from_numpy(rhs).to(dev)
+        sol = torch.full((N,), float("nan"), dtype=torch.float64, device=dev)
+        torch.cuda.synchronize()
+        k, rc = swm.jacobi_noalloc(nx, ny, *[p.data_ptr() for p in planes], cD.data_ptr(),
+                                   b.data_ptr(), sol.data_ptr(), block=block)
+        assert (k, rc) == (k_ref, rc_ref), call
+        assert np.array_equal(sol.cpu().numpy(), ref), call
+    s.close()
