@@ -183,6 +183,12 @@ static void host_bathy_grad(const swm_params& p, double x, double y, double* bx,
   }
 }
 
+// The split and FMA forms use the reciprocal Patankar weights and the 1/Diagonal
+// stencil Jacobi; the FP64 form keeps every division of the reference.
+static bool fast_patankar(const swm_params& p) {
+  return p.precision != SWM_PREC_FP64 && p.solver == SWM_SOLVER_STENCIL;
+}
+
 static int jacobi_block_of(const swm_params& p) {
   if (p.solver == SWM_SOLVER_CSR) return 1;
   return p.jacobi_block > 0 ? p.jacobi_block : 4;
@@ -276,6 +282,9 @@ static int enqueue_step(swm_solver* s) {
       aa.csr_mass = s->csr_mass;
       aa.csr_diag = s->csr_diag;
       aa.rhs_out = compat ? s->rhs_compat : nullptr;
+      aa.fast = fast_patankar(s->p) ? 1 : 0;
+      aa.inv_dx = 1.0 / s->gr.dx;
+      aa.inv_dy = 1.0 / s->gr.dy;
       prof_mark(s, 1);
       CK(launch_assemble(aa, csr, s->stream));
       prof_mark(s, -1);
@@ -300,6 +309,7 @@ static int enqueue_step(swm_solver* s) {
       ja.out = last ? s->h : s->hbuf[m - 1][k & 1];
       ja.ctl = s->ctl;
       ja.block = jacobi_block_of(s->p);
+      ja.recip = fast_patankar(s->p) ? 1 : 0;
       ja.spin_limit = 1LL << 26;
       prof_mark(s, 2);
       CK(launch_jacobi(ja, csr, s->jac_blocks, s->stream));
@@ -556,7 +566,7 @@ int swm_create(const swm_params* p, swm_handle* out) {
         cudaSuccess)
       return cleanup(fail(SWM_ERR_CUDA, "bathymetry table upload failed"));
   }
-  s->jac_blocks = jacobi_grid_blocks(csr, jacobi_block_of(s->p), s->device);
+  s->jac_blocks = jacobi_grid_blocks(csr, jacobi_block_of(s->p), s->device, fast_patankar(s->p));
   if (s->jac_blocks < 1) return cleanup(fail(SWM_ERR_CUDA, "Jacobi kernel cannot be resident"));
   // the RHS kernels' shared-memory attribute is set on first launch
   if (cudaDeviceSynchronize() != cudaSuccess)
@@ -914,7 +924,7 @@ int swm_debug_jacobi(swm_handle s, const double* mass, const double* diag, const
       pl[N + k] = mass[5 * k + 1];
       pl[2 * N + k] = mass[5 * k + 3];
       pl[3 * N + k] = mass[5 * k + 4];
-      pl[4 * N + k] = diag[k];
+      pl[4 * N + k] = fast_patankar(s->p) ? 1.0 / diag[k] : diag[k];
     }
     CK(cudaMemcpy(s->cS, pl.data(), N * sizeof(double), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(s->cW, pl.data() + N, N * sizeof(double), cudaMemcpyHostToDevice));
@@ -944,6 +954,7 @@ int swm_debug_jacobi(swm_handle s, const double* mass, const double* diag, const
   ja.out = out;
   ja.ctl = s->ctl;
   ja.block = jacobi_block_of(s->p);
+  ja.recip = fast_patankar(s->p) ? 1 : 0;
   ja.spin_limit = 1LL << 26;
   CK(launch_jacobi(ja, csr, s->jac_blocks, s->stream));
   CK(cudaStreamSynchronize(s->stream));

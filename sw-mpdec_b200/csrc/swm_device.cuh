@@ -176,6 +176,9 @@ __device__ __forceinline__ void cons_to_prim(double h, double hu, double hv, dou
 // ht = tangential); the reference's rotations by n=(1,0)/(0,1) and t=(0,1)/(-1,0)
 // multiply by exact 0 and +-1, so an x face passes (h,u,v) and a y face (h,v,u)
 // with the tangential component mapped back.
+// LAM32 (split form): the bound lam only scales the jump term lam*(UR-UL), so it is
+// formed from FP32 square roots; the fluxes themselves stay FP64.
+template <bool LAM32 = false>
 __device__ __forceinline__ void rusanov(double g, double hL, double nL, double tL, double hR,
                                         double nR, double tR, double& F0, double& F1, double& F2) {
   double FL0 = hL * nL;
@@ -184,8 +187,14 @@ __device__ __forceinline__ void rusanov(double g, double hL, double nL, double t
   double FR0 = hR * nR;
   double FR1 = hR * (nR * nR) + 0.5 * g * (hR * hR);
   double FR2 = hR * nR * tR;
-  double fastL = nL + sqrt(g * hL), fastR = nR + sqrt(g * hR);
-  double lam = dmax(fabs(fastL), fabs(fastR));
+  double lam;
+  if (LAM32) {
+    float fl = (float)nL + sqrtf((float)(g * hL)), fr = (float)nR + sqrtf((float)(g * hR));
+    lam = (double)fmaxf(fabsf(fl), fabsf(fr));
+  } else {
+    double fastL = nL + sqrt(g * hL), fastR = nR + sqrt(g * hR);
+    lam = dmax(fabs(fastL), fabs(fastR));
+  }
   F0 = 0.5 * ((FL0 + FR0) - lam * (hR - hL));
   F1 = 0.5 * ((FL1 + FR1) - lam * (hR * nR - hL * nL));
   F2 = 0.5 * ((FL2 + FR2) - lam * (hR * tR - hL * tL));

@@ -222,6 +222,13 @@ __device__ __forceinline__ double hp_read(const AssembleArgs& a, int m, int i, i
   return a.hp[m][(size_t)j * a.nx + i];
 }
 
+// 2h/(h^2 + max(h^2, MIN_DEPTH)), so that PATANKAR_DIV(p, h) = p * patankar_weight(h)
+__device__ __forceinline__ double patankar_weight(double h) {
+  if (h < kMinDepth) return 0.;
+  return 2. * h / (h * h + dmax(h * h, kMinDepth));
+}
+
+template <bool FAST>
 __global__ void assemble_kernel(const AssembleArgs a, bool csr) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y;
@@ -248,10 +255,13 @@ __global__ void assemble_kernel(const AssembleArgs a, bool csr) {
   // For a face flux f only one of P = max(f,0)/len and Q = -min(f,0)/len is non-zero,
   // and PATANKAR_DIV of a zero entry is a zero that leaves Mass/Diagonal unchanged, so
   // only the non-zero entry is formed; the non-zero updates keep the reference's order.
+  const double wK = FAST ? patankar_weight(hK) : 0.;
 #pragma unroll
   for (int nb = 0; nb < 4; ++nb) {
     const double hL = hp_read(a, m, ni[nb], nj[nb]);
     const double len = (nb == 0 || nb == 3) ? a.dy : a.dx;
+    const double ilen = (nb == 0 || nb == 3) ? a.inv_dy : a.inv_dx;
+    const double wL = FAST ? patankar_weight(hL) : 0.;
     for (int r = 0; r < ms; ++r) {
       double f;
       if (nb == 0)
@@ -263,7 +273,21 @@ __global__ void assemble_kernel(const AssembleArgs a, bool csr) {
       else
         f = -a.fym[r][(size_t)(j + 1) * nx + i];
       const double th = a.theta[r];
-      if (f > 0.) {  // production P_KL = f/len
+      if (FAST) {
+        if (f > 0.) {
+          const double P = f * ilen;
+          if (th > 0.)
+            M[nb] = M[nb] - dt * th * (P * wL);
+          else
+            D = D - dt * th * (P * wK);
+        } else if (f < 0.) {
+          const double Q = -f * ilen;
+          if (th > 0.)
+            D = D + dt * th * (Q * wK);
+          else
+            M[nb] = M[nb] + dt * th * (Q * wL);
+        }
+      } else if (f > 0.) {  // production P_KL = f/len
         const double P = f / len;
         if (th > 0.)
           M[nb] = M[nb] - dt * th * (patankar_div(P, hL));
@@ -292,14 +316,17 @@ __global__ void assemble_kernel(const AssembleArgs a, bool csr) {
     a.cW[k] = M[1];
     a.cE[k] = M[2];
     a.cN[k] = M[3];
-    a.cD[k] = D;
+    a.cD[k] = FAST ? 1.0 / D : D;  // the fast stencil solver multiplies by 1/Diagonal
   }
   if (a.rhs_out) a.rhs_out[k] = hp_read(a, 0, i, j);  // rhs = hp(1,.) (timediscretization.f90:887)
 }
 
 cudaError_t launch_assemble(const AssembleArgs& a, bool csr, cudaStream_t s) {
   dim3 blk(128), grd((a.nx + 127) / 128, a.ny);
-  assemble_kernel<<<grd, blk, 0, s>>>(a, csr);
+  if (a.fast && !csr)
+    assemble_kernel<true><<<grd, blk, 0, s>>>(a, csr);
+  else
+    assemble_kernel<false><<<grd, blk, 0, s>>>(a, csr);
   return cudaGetLastError();
 }
 
@@ -383,7 +410,7 @@ __device__ __forceinline__ int wrap_near(int g, int n) {
 // JBX x JBY block of cells plus a TB-cell halo in shared memory; sweep t updates
 // the region shrunk by t, so after Tp sweeps the tile interior holds x^{k+Tp},
 // bit-identical to Tp global sweeps.  Warps own rows, lanes own columns.
-template <int TB>
+template <int TB, bool RECIP>
 __device__ void stencil_pass(const JacobiArgs& a, const double* xin, double* xout, int Tp,
                              bool first, Acc& acc, double* sm) {
   using G = JTile<TB>;
@@ -464,7 +491,8 @@ __device__ void stencil_pass(const JacobiArgs& a, const double* xin, double* xou
             p = __dadd_rn(p, __dmul_rn(sW[c], xp[c - 1]));
             p = __dadd_rn(p, __dmul_rn(sE[c], xp[c + 1]));
             p = __dadd_rn(p, __dmul_rn(sN[c], xp[c + HX]));
-            const double xv = __ddiv_rn(__dsub_rn(sB[c], p), sD[c]);
+            const double xv = RECIP ? __dmul_rn(__dsub_rn(sB[c], p), sD[c])
+                                    : __ddiv_rn(__dsub_rn(sB[c], p), sD[c]);
             xn[c] = xv;
             if (row_in && lx >= TB && lx < TB + JBX && i0 + lx - TB < nx)
               acc_put(acc.v[t], fabs(__dsub_rn(xv, xp[c])));
@@ -516,7 +544,7 @@ __device__ __forceinline__ void acc_reduce(Acc& acc, unsigned long long (*s_acc)
     }
 }
 
-template <int TB, bool CSR>
+template <int TB, bool CSR, bool RECIP>
 __global__ void __launch_bounds__(JNT, 2) jacobi_kernel(const JacobiArgs a) {
   extern __shared__ __align__(16) double jsm[];
   __shared__ unsigned long long s_acc[kMaxBlock + 1][3];
@@ -544,7 +572,7 @@ __global__ void __launch_bounds__(JNT, 2) jacobi_kernel(const JacobiArgs a) {
     if (CSR)
       csr_pass(a, xin, xout, first, acc);
     else
-      stencil_pass<TB>(a, xin, xout, Tp, first, acc, jsm);
+      stencil_pass<TB, RECIP>(a, xin, xout, Tp, first, acc, jsm);
     acc_reduce<TB>(acc, s_acc);
     __syncthreads();
     const int slot = p % kResSlots;
@@ -588,7 +616,7 @@ __global__ void __launch_bounds__(JNT, 2) jacobi_kernel(const JacobiArgs a) {
         for (int q = threadIdx.x; q < (kMaxBlock + 1) * 3; q += blockDim.x)
           (&s_acc[0][0])[q] = 0ull;
         __syncthreads();
-        stencil_pass<TB>(a, xin, xout, stop, false, acc, jsm);
+        stencil_pass<TB, RECIP>(a, xin, xout, stop, false, acc, jsm);
         acc_reduce<TB>(acc, s_acc);
         if (!grid_barrier(ctl, a.spin_limit, &s_ok)) return;
         if (blockIdx.x == 0) {
@@ -625,35 +653,40 @@ __global__ void __launch_bounds__(JNT, 2) jacobi_kernel(const JacobiArgs a) {
   }
 }
 
-template <int TB, bool CSR>
+template <int TB, bool CSR, bool RECIP>
 static const void* jacobi_fn() {
-  return reinterpret_cast<const void*>(&jacobi_kernel<TB, CSR>);
+  return reinterpret_cast<const void*>(&jacobi_kernel<TB, CSR, RECIP>);
 }
 
-static const void* pick_jacobi(bool csr, int block, size_t* smem) {
-  if (csr) {
-    *smem = 0;
-    return jacobi_fn<1, true>();
-  }
+template <bool RECIP>
+static const void* pick_stencil(int block, size_t* smem) {
   if (block <= 1) {
     *smem = JTile<1>::bytes;
-    return jacobi_fn<1, false>();
+    return jacobi_fn<1, false, RECIP>();
   }
   if (block <= 2) {
     *smem = JTile<2>::bytes;
-    return jacobi_fn<2, false>();
+    return jacobi_fn<2, false, RECIP>();
   }
   if (block <= 4) {
     *smem = JTile<4>::bytes;
-    return jacobi_fn<4, false>();
+    return jacobi_fn<4, false, RECIP>();
   }
   *smem = JTile<8>::bytes;
-  return jacobi_fn<8, false>();
+  return jacobi_fn<8, false, RECIP>();
 }
 
-int jacobi_grid_blocks(bool csr, int block, int device) {
+static const void* pick_jacobi(bool csr, int block, bool recip, size_t* smem) {
+  if (csr) {
+    *smem = 0;
+    return jacobi_fn<1, true, false>();
+  }
+  return recip ? pick_stencil<true>(block, smem) : pick_stencil<false>(block, smem);
+}
+
+int jacobi_grid_blocks(bool csr, int block, int device, bool recip) {
   size_t smem = 0;
-  const void* fn = pick_jacobi(csr, block, &smem);
+  const void* fn = pick_jacobi(csr, block, recip, &smem);
   if (smem > 48 * 1024)
     cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int per_sm = 0;
@@ -667,7 +700,7 @@ int jacobi_grid_blocks(bool csr, int block, int device) {
 
 cudaError_t launch_jacobi(const JacobiArgs& a, bool csr, int grid_blocks, cudaStream_t s) {
   size_t smem = 0;
-  const void* fn = pick_jacobi(csr, a.block, &smem);
+  const void* fn = pick_jacobi(csr, a.block, a.recip != 0, &smem);
   int n = a.nx * a.ny;
   int blocks = grid_blocks;
   if (csr) {

@@ -51,6 +51,10 @@ struct AssembleArgs {
   double* csr_mass;
   double* csr_diag;
   double* rhs_out;        // nullable: rhs = hp(1,.) (needed when hp is read through compat2)
+  // split form: PATANKAR_DIV from one reciprocal per depth, P/D by 1/dx, and the
+  // stencil diagonal stored as 1/Diagonal (not bit-identical to the reference order)
+  int fast;
+  double inv_dx, inv_dy;
 };
 
 struct JacobiArgs {
@@ -75,6 +79,7 @@ struct JacobiArgs {
   double* out;            // final iterate destination
   JacobiCtl* ctl;
   int block;              // sweeps per pass (stencil)
+  int recip;              // stencil: cD holds 1/Diagonal (split form)
   long long spin_limit;   // grid-barrier watchdog
 };
 
@@ -96,7 +101,7 @@ size_t rhs_smem_bytes(int mode);
 cudaError_t launch_dt(const DtArgs& a, cudaStream_t s);
 cudaError_t launch_assemble(const AssembleArgs& a, bool csr, cudaStream_t s);
 cudaError_t launch_jacobi(const JacobiArgs& a, bool csr, int grid_blocks, cudaStream_t s);
-int jacobi_grid_blocks(bool csr, int block, int device);
+int jacobi_grid_blocks(bool csr, int block, int device, bool recip = false);
 cudaError_t launch_ghosted_to_planes(const double* G, int nx, int ny, double* h, double* hu,
                                      double* hv, cudaStream_t s);
 cudaError_t launch_planes_to_ghosted(const double* h, const double* hu, const double* hv, int nx,

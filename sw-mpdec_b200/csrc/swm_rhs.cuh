@@ -186,7 +186,7 @@ __global__ void __launch_bounds__(RHS_NT, 2) rhs_kernel(const RhsArgs a) {
       for (int g = 0; g < 4; ++g) {
         const int L = rr * FW + ff, R = rr * FW + ff + 1;
         double F0, F1, F2;
-        rusanov(gr.g, sW[((1 * 3 + 0) * 4 + g) * WC + L], sW[((1 * 3 + 1) * 4 + g) * WC + L],
+        rusanov<MODE == 1>(gr.g, sW[((1 * 3 + 0) * 4 + g) * WC + L], sW[((1 * 3 + 1) * 4 + g) * WC + L],
                 sW[((1 * 3 + 2) * 4 + g) * WC + L], sW[((0 * 3 + 0) * 4 + g) * WC + R],
                 sW[((0 * 3 + 1) * 4 + g) * WC + R], sW[((0 * 3 + 2) * 4 + g) * WC + R], F0, F1,
                 F2);
@@ -278,7 +278,7 @@ __global__ void __launch_bounds__(RHS_NT, 2) rhs_kernel(const RhsArgs a) {
         const int L = fr * TX + cc, R = (fr + 1) * TX + cc;
         double F0, F1, F2;
         // normal = v (var 2), tangential = u (var 1)
-        rusanov(gr.g, sW[((1 * 3 + 0) * 4 + g) * WC + L], sW[((1 * 3 + 2) * 4 + g) * WC + L],
+        rusanov<MODE == 1>(gr.g, sW[((1 * 3 + 0) * 4 + g) * WC + L], sW[((1 * 3 + 2) * 4 + g) * WC + L],
                 sW[((1 * 3 + 1) * 4 + g) * WC + L], sW[((0 * 3 + 0) * 4 + g) * WC + R],
                 sW[((0 * 3 + 2) * 4 + g) * WC + R], sW[((0 * 3 + 1) * 4 + g) * WC + R], F0, F1,
                 F2);
