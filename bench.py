@@ -195,6 +195,7 @@ def main():
     ap.add_argument("--block", type=int, default=4)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--n", type=int, default=2048)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
@@ -282,6 +283,42 @@ def main():
                "ms_per_step": ms_e2e / args.steps}
         s.close()
 
+    # ensemble: 256 problems of uneven size in one batch (split, autotuned Jacobi
+    # sweeps per pass); under torchrun the problem list is sharded across ranks
+    ens = None
+    if not args.no_ensemble:
+        members = cases.ensemble(seed=0)
+        sizes = [m["nx"] * m["ny"] for m in members]
+        mine = replicas.shard(sizes, rank, world)
+        plist = [swm.make_params(m["nx"], m["ny"], m["x0"], m["x1"], g=m["g"], cfl=m["cfl"],
+                                 bathy_flag=m["bathy_flag"], bathy_par=m["bathy_par"],
+                                 precision="split", solver="stencil", jacobi_block=0,
+                                 device=local) for m in (members[i] for i in mine)]
+        bt = swm.Batch(plist)
+        for k, i in enumerate(mine):
+            bt.set_planes(k, cases.cell_averages(members[i]))
+        for _ in range(max(args.warmup, 1)):  # the first step also picks sweeps per pass
+            bt.step()
+        barrier()
+        st = torch.cuda.ExternalStream(bt.stream())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(args.steps):
+            bt.step()
+        e1.record(st)
+        torch.cuda.synchronize()
+        ms_ens, cell_steps = replicas.aggregate(e0.elapsed_time(e1), bt.cells() * args.steps,
+                                                dist, device="cuda")
+        blk, tot, last = bt.stats()
+        ens = {"workload": "256 problems, sides log-uniform in [64,512], vortex / dam break / "
+                           "Gaussian lake families, seed 0, split precision",
+               "value": cell_steps / (ms_ens * 1e-3), "unit": "cell-steps/s",
+               "cells": int(sum(sizes)), "ms_per_step": ms_ens / args.steps,
+               "jacobi_block_autotuned": blk,
+               "jacobi_iters_per_step_max": int(last.sum(axis=0).max()),
+               "launches_per_step": 1 + 13 * 3}
+        bt.close()
+
     if rank != 0:
         if dist is not None:
             dist.destroy_process_group()
@@ -335,6 +372,7 @@ def main():
         "gpu_launches": launches * args.steps,
         "clocks": clocks,
         "e2e": e2e,
+        "ensemble": ens,
     }
     if not args.no_cpu:
         try:

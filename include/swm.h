@@ -184,8 +184,13 @@ SWM_API int swm_jacobi_noalloc(int nx, int ny, const double *cS, const double *c
 
 /* ---- batched ensembles ---- */
 typedef struct swm_batch *swm_batch_handle;
-/* n problems of independent size and parameters, stepped together: one
- * persistent launch per phase covers every problem's tiles. */
+/* n problems of independent size and parameters, stepped together: one launch
+ * per phase covers every problem's tiles (the Jacobi solve is one cooperative
+ * launch in which each problem keeps its own stop rule), and the whole step is a
+ * CUDA graph.  All problems share precision and jacobi_block (taken from p[0]);
+ * mPDeC5 only, no well-balanced reference; the stencil solver is always used.
+ * jacobi_block = 0 lets the first step time 2, 4 and 8 sweeps per pass on the
+ * initial state and keep the fastest. */
 SWM_API int swm_batch_create(int n, const swm_params *p, swm_batch_handle *out);
 SWM_API int swm_batch_destroy(swm_batch_handle b);
 SWM_API int swm_batch_set_planes(swm_batch_handle b, int i, const double *planes);
@@ -194,6 +199,13 @@ SWM_API int swm_batch_get_planes(swm_batch_handle b, int i, double *planes);
  * the device); dt_out[n] (nullable) receives the steps taken. */
 SWM_API int swm_batch_step(swm_batch_handle b, double *dt_out);
 SWM_API int swm_batch_cells(swm_batch_handle b, long long *cells);
+/* Sweeps per Jacobi pass in use (chosen by the first step when jacobi_block was 0),
+ * Jacobi sweeps summed over all steps and problems, and (nullable) the sweeps of
+ * the last step, [13][n] (solve-major). */
+SWM_API int swm_batch_get_stats(swm_batch_handle b, int *jacobi_block, long long *iters_total,
+                                int *last_iters);
+/* The cudaStream_t the ensemble launches on (for CUDA-event timing by the caller). */
+SWM_API int swm_batch_get_stream(swm_batch_handle b, void **stream);
 
 #ifdef __cplusplus
 }

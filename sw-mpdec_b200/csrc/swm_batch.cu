@@ -1,73 +1,607 @@
-// swm_batch.cu -- batched ensembles of independent problems.
-// First form: one handle per problem, stepped in sequence on the device, each
-// with its own dt.  (The persistent multi-problem kernels replace this path.)
-#include <cstdlib>
+// swm_batch.cu -- ensembles of independent problems on uneven grids.
+//
+// Every phase of an mPDeC5 step is one launch covering all problems: the batched
+// dt reduction (per-problem TimeStep, computed on the device), 13 batched RHS
+// launches (one CTA per (problem, tile)), 13 batched assemblies and 13 cooperative
+// Jacobi launches in which each problem keeps its own stop rule.  The whole step
+// is captured once into a CUDA graph.  jacobi_block = 0 lets the first step try
+// the candidate sweeps-per-pass on the initial state and keep the fastest
+// (results do not depend on it: every candidate produces the same iterates).
+#include <cmath>
+#include <cstring>
+#include <string>
 #include <vector>
 
 #include "../../include/swm.h"
+#include "swm_kernels.cuh"
 
-struct swm_batch {
-  std::vector<swm_handle> h;
-  std::vector<long long> cells;
+using namespace swm;
+
+namespace swm {
+void set_last_error(const char* msg);
+}
+
+namespace {
+
+int bfail(int code, const std::string& msg) {
+  swm::set_last_error(msg.c_str());
+  return code;
+}
+
+#define BCK(call)                                                                        \
+  do {                                                                                   \
+    cudaError_t e_ = (call);                                                             \
+    if (e_ != cudaSuccess)                                                               \
+      return bfail(SWM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));    \
+  } while (0)
+
+// thetaDeC (timediscretization.f90:491-506), rows m = 1..4
+const double kTh5[4][4] = {
+    {0.0000000000000000000, 0.0000000000000000000, 0.0000000000000000000, 0.0000000000000000000},
+    {0.1103005664791649049, 0.1896994335208351257, -0.0339073642291439076, 0.0103005664791649201},
+    {0.0730327668541684294, 0.4505740308958107176, 0.2269672331458314485, -0.0269672331458315692},
+    {0.0833333333333333287, 0.4166666666666666852, 0.4166666666666666852, 0.0833333333333333287}};
+const int kSolves = 13;    // mPDeC5: 3 substeps x 4 corrections + 1
+const int kRhsSets = 7;    // U^n, and Ua(m) for m = 2..4 at both correction parities
+const int kCandidates[3] = {2, 4, 8};
+
+struct BProblem {
+  swm_params p{};
+  int nx = 0, ny = 0;
+  size_t N = 0;
+  Grid gr{};
+  double *h = nullptr, *hu = nullptr, *hv = nullptr;
+  double* hbuf[4][2] = {};
+  double* hum[4] = {};
+  double* hvm[4] = {};
+  double* fu[4] = {};
+  double* fv[4] = {};
+  double* fxm[4] = {};
+  double* fym[4] = {};
+  double *cS = nullptr, *cW = nullptr, *cE = nullptr, *cN = nullptr, *cD = nullptr;
+  double *xa = nullptr, *xb = nullptr;
+  double *gex = nullptr, *gey = nullptr, *bgrad = nullptr;
+  double* save[3] = {};  // state copy used while tuning
 };
 
-extern "C" {
+void quad(double qn[4], double qw[4]) {  // mesh.f90:127-129
+  qw[0] = (18. - sqrt(30.)) / 72.;
+  qw[1] = (18. + sqrt(30.)) / 72.;
+  qw[2] = (18. + sqrt(30.)) / 72.;
+  qw[3] = (18. - sqrt(30.)) / 72.;
+  qn[0] = -(0.5 * sqrt(3. / 7. + 2. / 7. * sqrt(6. / 5.)));
+  qn[1] = -(0.5 * sqrt(3. / 7. - 2. / 7. * sqrt(6. / 5.)));
+  qn[2] = 0.5 * sqrt(3. / 7. - 2. / 7. * sqrt(6. / 5.));
+  qn[3] = 0.5 * sqrt(3. / 7. + 2. / 7. * sqrt(6. / 5.));
+}
 
-int swm_batch_create(int n, const swm_params* p, swm_batch_handle* out) {
-  if (!out || !p || n < 1) return SWM_ERR_PARAM;
-  *out = nullptr;
-  swm_batch* b = new swm_batch();
-  for (int i = 0; i < n; ++i) {
-    swm_handle h = nullptr;
-    int rc = swm_create(&p[i], &h);
-    if (rc) {
-      swm_batch_destroy(b);
-      return rc;
+double gpx(double x0, double h, int c, double q) {
+  double node = x0 + ((double)c) * h;
+  double bary = node + 0.5 * h;
+  return bary + q * h;
+}
+
+// Bathymetry_X/_Y (equation.f90:451-509) and the Gaussian case, on the host.
+void bgrad_host(const swm_params& p, double x, double y, double* bx, double* by) {
+  const double PI = acos(-1.0);
+  *bx = 0.;
+  *by = 0.;
+  if (p.bathy_flag == SWM_BATHY_SINCOS) {
+    *bx = 0.1 * 2. * PI * cos(2. * PI * x) * cos(2. * PI * y);
+    *by = -(0.1 * 2. * PI * sin(2. * PI * x) * sin(2. * PI * y));
+  } else if (p.bathy_flag == SWM_BATHY_BUMP) {
+    double r2 = x * x + y * y;
+    if (r2 < 1) {
+      double d = 1.0 - r2, e = exp(1.0 - 1.0 / d);
+      *bx = -(2.0 * x / (d * d) * e);
+      *by = -(2.0 * y / (d * d) * e);
     }
-    b->h.push_back(h);
-    b->cells.push_back((long long)p[i].nx * p[i].ny);
+  } else if (p.bathy_flag == SWM_BATHY_GAUSS) {
+    double dxv = x - p.bathy_par[2], dyv = y - p.bathy_par[4];
+    double e = exp(-(p.bathy_par[1] * (dxv * dxv) + p.bathy_par[3] * (dyv * dyv)));
+    double B = p.bathy_par[0] * e;
+    *bx = (-2.0 * p.bathy_par[1] * dxv) * B;
+    *by = (-2.0 * p.bathy_par[3] * dyv) * B;
   }
-  *out = b;
+}
+
+}  // namespace
+
+struct swm_batch {
+  std::vector<BProblem> pr;
+  int n = 0, device = 0, precision = 0, block = 4;
+  bool autotune = false, fast = false;
+  cudaStream_t stream = nullptr;
+  std::vector<void*> allocs;
+  RhsArgs* d_rhs = nullptr;        // [kRhsSets][n]
+  AssembleArgs* d_asm = nullptr;   // [kSolves][n]
+  JacobiArgs* d_jac = nullptr;     // [kSolves][n]
+  int4* d_rhs_work = nullptr;
+  int nrhs = 0;
+  int2* d_cells = nullptr;         // 128-cell blocks (problem, first cell)
+  int ncellblk = 0;
+  int2* d_tiles = nullptr;         // Jacobi tiles (problem, tile)
+  int ntiles = 0;
+  DtBatchDesc* d_dtd = nullptr;
+  double* d_dt = nullptr;
+  unsigned long long* d_lam = nullptr;
+  int* d_bad = nullptr;
+  JacBatchState* d_st = nullptr;
+  JacBatchCtl* d_ctl = nullptr;
+  int* d_iters = nullptr;          // [kSolves][n]
+  int jac_blocks[9] = {};
+  cudaGraphExec_t graph = nullptr;
+  // host mirrors
+  std::vector<double> h_dt;
+  std::vector<int> h_iters, h_bad;
+  long long cells = 0;
+  long long iters_total = 0;
+  bool have_state = false;
+
+  template <typename T>
+  int alloc(T** ptr, size_t count) {
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, count * sizeof(T) + 256);
+    if (e != cudaSuccess) return bfail(SWM_ERR_ALLOC, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    cudaMemset(q, 0, count * sizeof(T) + 256);
+    allocs.push_back(q);
+    *ptr = static_cast<T*>(q);
+    return SWM_OK;
+  }
+};
+
+static int batch_valid(int n, const swm_params* p) {
+  if (n < 1 || !p) return bfail(SWM_ERR_PARAM, "n >= 1 problems required");
+  for (int i = 0; i < n; ++i) {
+    const swm_params& q = p[i];
+    if (q.nx < 3 || q.ny < 3) return bfail(SWM_ERR_PARAM, "nx, ny must be >= 3");
+    if (q.timescheme != 5) return bfail(SWM_ERR_PARAM, "ensembles run mPDeC5 (timescheme 5)");
+    if (q.well_balanced) return bfail(SWM_ERR_PARAM, "ensembles take no well-balanced reference");
+    if (q.precision != p[0].precision) return bfail(SWM_ERR_PARAM, "one precision per ensemble");
+    if (q.precision < 0 || q.precision > 2) return bfail(SWM_ERR_PARAM, "unknown precision");
+    if (q.bathy_flag < 0 || q.bathy_flag > 3) return bfail(SWM_ERR_PARAM, "unknown bathymetry");
+    if (q.jacobi_maxiter < 1 || !(q.jacobi_tol >= 0.0)) return bfail(SWM_ERR_PARAM, "Jacobi limits");
+    if (!(q.g > 0.0) || !(q.cfl > 0.0) || q.x1[0] == q.x0[0] || q.x1[1] == q.x0[1])
+      return bfail(SWM_ERR_PARAM, "invalid domain, g or cfl");
+  }
+  if (p[0].jacobi_block < 0 || p[0].jacobi_block > kMaxBlock)
+    return bfail(SWM_ERR_PARAM, "jacobi_block must be in 0..8");
   return SWM_OK;
 }
 
+// Per-problem arrays (same roles as in the single-grid handle).
+static int batch_alloc_problem(swm_batch* b, BProblem& q) {
+  const size_t N = q.N, nfx = (size_t)(q.nx + 1) * q.ny, nfy = (size_t)q.nx * (q.ny + 1);
+  int rc = 0;
+#define BA(ptr, cnt) \
+  if (!rc) rc = b->alloc(&(ptr), (cnt))
+  BA(q.h, N);
+  BA(q.hu, N);
+  BA(q.hv, N);
+  for (int m = 1; m < 4; ++m) {
+    BA(q.hbuf[m][0], N);
+    BA(q.hbuf[m][1], N);
+    BA(q.hum[m], N);
+    BA(q.hvm[m], N);
+  }
+  for (int r = 0; r < 4; ++r) {
+    BA(q.fu[r], N);
+    BA(q.fv[r], N);
+    BA(q.fxm[r], nfx);
+    BA(q.fym[r], nfy);
+  }
+  BA(q.cS, N);
+  BA(q.cW, N);
+  BA(q.cE, N);
+  BA(q.cN, N);
+  BA(q.cD, N);
+  BA(q.xa, N);
+  BA(q.xb, N);
+#undef BA
+  if (rc) return rc;
+  const Grid& gr = q.gr;
+  if (q.p.bathy_flag == SWM_BATHY_GAUSS && q.p.precision != SWM_PREC_FP64) {
+    if ((rc = b->alloc(&q.gex, 4 * (size_t)q.nx)) || (rc = b->alloc(&q.gey, 4 * (size_t)q.ny)))
+      return rc;
+    std::vector<double> ex(4 * q.nx), ey(4 * q.ny);
+    for (int i = 0; i < q.nx; ++i)
+      for (int k = 0; k < 4; ++k) {
+        double d = gpx(gr.x0, gr.dx, i, gr.qn[k]) - gr.bp[2];
+        ex[4 * i + k] = exp(-(gr.bp[1] * (d * d)));
+      }
+    for (int j = 0; j < q.ny; ++j)
+      for (int k = 0; k < 4; ++k) {
+        double d = gpx(gr.y0, gr.dy, j, gr.qn[k]) - gr.bp[4];
+        ey[4 * j + k] = exp(-(gr.bp[3] * (d * d)));
+      }
+    BCK(cudaMemcpy(q.gex, ex.data(), sizeof(double) * ex.size(), cudaMemcpyHostToDevice));
+    BCK(cudaMemcpy(q.gey, ey.data(), sizeof(double) * ey.size(), cudaMemcpyHostToDevice));
+  } else if (q.p.bathy_flag > 0) {
+    if ((rc = b->alloc(&q.bgrad, 32 * N))) return rc;
+    std::vector<double> tab(32 * N);
+    for (int a = 0; a < 4; ++a)
+      for (int c = 0; c < 4; ++c)
+        for (int j = 0; j < q.ny; ++j)
+          for (int i = 0; i < q.nx; ++i) {
+            double bx, by;
+            bgrad_host(q.p, gpx(gr.x0, gr.dx, i, gr.qn[a]), gpx(gr.y0, gr.dy, j, gr.qn[c]), &bx,
+                       &by);
+            tab[((a * 4 + c) * 2 + 0) * N + (size_t)j * q.nx + i] = bx;
+            tab[((a * 4 + c) * 2 + 1) * N + (size_t)j * q.nx + i] = by;
+          }
+    BCK(cudaMemcpy(q.bgrad, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice));
+  }
+  return SWM_OK;
+}
+
+// RHS descriptor: input state (h, hu, hv) -> stage slot `slot`.
+static RhsArgs batch_rhs_desc(const BProblem& q, const double* h, const double* hu,
+                              const double* hv, int slot) {
+  RhsArgs a{};
+  a.gr = q.gr;
+  a.h = h;
+  a.hu = hu;
+  a.hv = hv;
+  a.ut_hu = q.fu[slot];
+  a.ut_hv = q.fv[slot];
+  a.fxm = q.fxm[slot];
+  a.fym = q.fym[slot];
+  a.gauss_ex = q.gex;
+  a.gauss_ey = q.gey;
+  a.bgrad = q.bgrad;
+  return a;
+}
+
+// Descriptor tables of the fixed step sequence (the same sequence enqueue_step issues).
+static int batch_tables(swm_batch* b) {
+  const int n = b->n;
+  std::vector<RhsArgs> rhs((size_t)kRhsSets * n);
+  std::vector<AssembleArgs> as((size_t)kSolves * n);
+  std::vector<JacobiArgs> ja((size_t)kSolves * n);
+  for (int i = 0; i < n; ++i) {
+    const BProblem& q = b->pr[i];
+    rhs[i] = batch_rhs_desc(q, q.h, q.hu, q.hv, 0);
+    for (int par = 0; par < 2; ++par)
+      for (int m = 2; m <= 4; ++m)
+        rhs[(size_t)(1 + par * 3 + (m - 2)) * n + i] =
+            batch_rhs_desc(q, q.hbuf[m - 1][par], q.hum[m - 1], q.hvm[m - 1], m - 1);
+    int solve = 0;
+    for (int k = 1; k <= 5; ++k) {
+      const int mlo = (k == 5) ? 4 : 2;
+      for (int m = mlo; m <= 4; ++m, ++solve) {
+        const bool last = (k == 5);
+        AssembleArgs& aa = as[(size_t)solve * n + i];
+        aa.nx = q.nx;
+        aa.ny = q.ny;
+        aa.dx = q.gr.dx;
+        aa.dy = q.gr.dy;
+        aa.m = m;
+        aa.msteps = 4;
+        for (int r = 0; r < 4; ++r) aa.theta[r] = kTh5[m - 1][r];
+        aa.dt = b->d_dt + i;
+        aa.hu_n = q.hu;
+        aa.hv_n = q.hv;
+        for (int r = 0; r < 4; ++r) {
+          const int slot = (k == 1) ? 0 : r;
+          aa.fu[r] = q.fu[slot];
+          aa.fv[r] = q.fv[slot];
+          aa.fxm[r] = q.fxm[slot];
+          aa.fym[r] = q.fym[slot];
+          aa.hp[r] = (r == 0 || k == 1) ? q.h : q.hbuf[r][(k - 1) & 1];
+        }
+        aa.hu_out = last ? q.hu : q.hum[m - 1];
+        aa.hv_out = last ? q.hv : q.hvm[m - 1];
+        aa.cS = q.cS;
+        aa.cW = q.cW;
+        aa.cE = q.cE;
+        aa.cN = q.cN;
+        aa.cD = q.cD;
+        aa.fast = b->fast ? 1 : 0;
+        aa.inv_dx = 1.0 / q.gr.dx;
+        aa.inv_dy = 1.0 / q.gr.dy;
+        JacobiArgs& jj = ja[(size_t)solve * n + i];
+        jj.nx = q.nx;
+        jj.ny = q.ny;
+        jj.maxiter = q.p.jacobi_maxiter;
+        residual_limbs_host(q.p.jacobi_tol * (double)q.N, jj.thresh);
+        jj.b = q.h;
+        jj.cS = q.cS;
+        jj.cW = q.cW;
+        jj.cE = q.cE;
+        jj.cN = q.cN;
+        jj.cD = q.cD;
+        jj.xa = q.xa;
+        jj.xb = q.xb;
+        jj.out = last ? q.h : q.hbuf[m - 1][k & 1];
+        jj.recip = b->fast ? 1 : 0;
+      }
+    }
+  }
+  BCK(cudaMemcpy(b->d_rhs, rhs.data(), sizeof(RhsArgs) * rhs.size(), cudaMemcpyHostToDevice));
+  BCK(cudaMemcpy(b->d_asm, as.data(), sizeof(AssembleArgs) * as.size(), cudaMemcpyHostToDevice));
+  BCK(cudaMemcpy(b->d_jac, ja.data(), sizeof(JacobiArgs) * ja.size(), cudaMemcpyHostToDevice));
+  return SWM_OK;
+}
+
+static cudaError_t batch_rhs(swm_batch* b, int set) {
+  const RhsArgs* d = b->d_rhs + (size_t)set * b->n;
+  if (b->precision == SWM_PREC_FP64) return launch_rhs_batch_exact(d, b->d_rhs_work, b->nrhs, b->stream);
+  return launch_rhs_batch_fast(b->precision == SWM_PREC_SPLIT ? 1 : 0, d, b->d_rhs_work, b->nrhs,
+                               b->stream);
+}
+
+// One mPDeC5 step of every problem (timediscretization.f90:458-566), dt per problem
+// from the batched TimeStep, all on b->stream.
+static int batch_enqueue(swm_batch* b, int block) {
+  BCK(cudaMemsetAsync(b->d_ctl, 0, sizeof(JacBatchCtl), b->stream));
+  BCK(launch_dt_batch(b->d_dtd, b->d_cells, b->ncellblk, b->n, b->d_lam, b->d_bad, b->d_dt,
+                      b->stream));
+  BCK(batch_rhs(b, 0));
+  int solve = 0;
+  for (int k = 1; k <= 5; ++k) {
+    const int mlo = (k == 5) ? 4 : 2;
+    for (int m = mlo; m <= 4; ++m, ++solve) {
+      BCK(launch_assemble_batch(b->d_asm + (size_t)solve * b->n, b->d_cells, b->ncellblk, b->fast,
+                                b->stream));
+      JacobiBatchArgs ja{};
+      ja.descs = b->d_jac + (size_t)solve * b->n;
+      ja.tiles = b->d_tiles;
+      ja.ntiles = b->ntiles;
+      ja.nprob = b->n;
+      ja.st = b->d_st;
+      ja.ctl = b->d_ctl;
+      ja.iters = b->d_iters + (size_t)solve * b->n;
+      ja.block = block;
+      ja.spin_limit = 1LL << 26;
+      BCK(launch_jacobi_batch(ja, b->jac_blocks[block], b->fast, b->stream));
+    }
+    if (k < 5)
+      for (int m = 2; m <= 4; ++m) BCK(batch_rhs(b, 1 + (k & 1) * 3 + (m - 2)));
+  }
+  return SWM_OK;
+}
+
+static int batch_graph(swm_batch* b) {
+  if (b->graph) return SWM_OK;
+  cudaGraph_t g = nullptr;
+  BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = batch_enqueue(b, b->block);
+  cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+  if (rc) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (e != cudaSuccess) return bfail(SWM_ERR_CUDA, cudaGetErrorString(e));
+  e = cudaGraphInstantiate(&b->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) {
+    b->graph = nullptr;
+    return bfail(SWM_ERR_CUDA, cudaGetErrorString(e));
+  }
+  return SWM_OK;
+}
+
+static int batch_copy_state(swm_batch* b, bool to_save) {
+  for (auto& q : b->pr) {
+    double* live[3] = {q.h, q.hu, q.hv};
+    for (int v = 0; v < 3; ++v) {
+      double* dst = to_save ? q.save[v] : live[v];
+      double* src = to_save ? live[v] : q.save[v];
+      BCK(cudaMemcpyAsync(dst, src, sizeof(double) * q.N, cudaMemcpyDeviceToDevice, b->stream));
+    }
+  }
+  return SWM_OK;
+}
+
+// Autotuner: time one step per candidate sweeps-per-pass on the initial state,
+// restore the state after each, keep the fastest.
+static int batch_tune(swm_batch* b) {
+  for (auto& q : b->pr)
+    for (int v = 0; v < 3; ++v)
+      if (!q.save[v]) {
+        int rc = b->alloc(&q.save[v], q.N);
+        if (rc) return rc;
+      }
+  int rc = batch_copy_state(b, true);
+  if (rc) return rc;
+  cudaEvent_t e0, e1;
+  BCK(cudaEventCreate(&e0));
+  BCK(cudaEventCreate(&e1));
+  float best = 1e30f;
+  int best_block = 4;
+  for (int c : kCandidates) {
+    for (int rep = 0; rep < 2; ++rep) {  // first repetition warms the kernels
+      BCK(cudaEventRecord(e0, b->stream));
+      if ((rc = batch_enqueue(b, c))) return rc;
+      BCK(cudaEventRecord(e1, b->stream));
+      BCK(cudaStreamSynchronize(b->stream));
+      if ((rc = batch_copy_state(b, false))) return rc;
+    }
+    float ms = 0.f;
+    BCK(cudaEventElapsedTime(&ms, e0, e1));
+    if (ms < best) {
+      best = ms;
+      best_block = c;
+    }
+  }
+  BCK(cudaStreamSynchronize(b->stream));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  b->block = best_block;
+  b->autotune = false;
+  return SWM_OK;
+}
+
+extern "C" {
+
 int swm_batch_destroy(swm_batch_handle b) {
   if (!b) return SWM_OK;
-  for (auto h : b->h) swm_destroy(h);
+  cudaSetDevice(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  for (void* q : b->allocs) cudaFree(q);
+  if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
   return SWM_OK;
 }
 
+int swm_batch_create(int n, const swm_params* p, swm_batch_handle* out) {
+  if (!out) return bfail(SWM_ERR_PARAM, "null handle pointer");
+  *out = nullptr;
+  int rc = batch_valid(n, p);
+  if (rc) return rc;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return bfail(SWM_ERR_CUDA, "no CUDA device available");
+  if (p[0].device < 0 || p[0].device >= ndev) return bfail(SWM_ERR_PARAM, "invalid device ordinal");
+  BCK(cudaSetDevice(p[0].device));
+  int major = 0;
+  cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, p[0].device);
+  if (major != 10) return bfail(SWM_ERR_UNSUPPORTED, "this build targets sm_100a (B200) only");
+  swm_batch* b = new swm_batch();
+  auto cleanup = [&](int code) {
+    swm_batch_destroy(b);
+    return code;
+  };
+  b->n = n;
+  b->device = p[0].device;
+  b->precision = p[0].precision;
+  b->fast = b->precision != SWM_PREC_FP64;
+  b->autotune = p[0].jacobi_block == 0;
+  b->block = b->autotune ? 4 : p[0].jacobi_block;
+  if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return cleanup(bfail(SWM_ERR_CUDA, "cudaStreamCreate failed"));
+  b->pr.resize(n);
+  std::vector<int4> rw;
+  std::vector<int2> cb, tl;
+  std::vector<DtBatchDesc> dd(n);
+  for (int i = 0; i < n; ++i) {
+    BProblem& q = b->pr[i];
+    q.p = p[i];
+    q.nx = p[i].nx;
+    q.ny = p[i].ny;
+    q.N = (size_t)q.nx * q.ny;
+    Grid& gr = q.gr;
+    gr.nx = q.nx;
+    gr.ny = q.ny;
+    gr.x0 = p[i].x0[0];
+    gr.y0 = p[i].x0[1];
+    gr.dx = fabs(fabs(p[i].x1[0] - p[i].x0[0])) / ((double)q.nx);
+    gr.dy = fabs(fabs(p[i].x1[1] - p[i].x0[1])) / ((double)q.ny);
+    gr.g = p[i].g;
+    gr.bathy = p[i].bathy_flag;
+    for (int k = 0; k < 5; ++k) gr.bp[k] = p[i].bathy_par[k];
+    quad(gr.qn, gr.qw);
+    for (int a = 0; a < 4; ++a)
+      for (int c = 0; c < 4; ++c) gr.wgp[a][c] = gr.qw[a] * gr.qw[c];
+    if ((rc = batch_alloc_problem(b, q))) return cleanup(rc);
+    for (int ty = 0; ty < (q.ny + RHS_TY - 1) / RHS_TY; ++ty)
+      for (int tx = 0; tx < (q.nx + RHS_TX - 1) / RHS_TX; ++tx)
+        rw.push_back(make_int4(i, tx * RHS_TX, ty * RHS_TY, 0));
+    for (size_t c0 = 0; c0 < q.N; c0 += 128) cb.push_back(make_int2(i, (int)c0));
+    const int jt = ((q.nx + 63) / 64) * ((q.ny + 15) / 16);  // Jacobi tiles (64 x 16)
+    for (int t = 0; t < jt; ++t) tl.push_back(make_int2(i, t));
+    dd[i] = DtBatchDesc{q.nx, q.ny, gr.g, p[i].cfl, gr.dx, gr.dy, q.h, q.hu, q.hv};
+    b->cells += (long long)q.N;
+  }
+  b->nrhs = (int)rw.size();
+  b->ncellblk = (int)cb.size();
+  b->ntiles = (int)tl.size();
+  if ((rc = b->alloc(&b->d_rhs, (size_t)kRhsSets * n)) || (rc = b->alloc(&b->d_asm, (size_t)kSolves * n)) ||
+      (rc = b->alloc(&b->d_jac, (size_t)kSolves * n)) || (rc = b->alloc(&b->d_rhs_work, rw.size())) ||
+      (rc = b->alloc(&b->d_cells, cb.size())) || (rc = b->alloc(&b->d_tiles, tl.size())) ||
+      (rc = b->alloc(&b->d_dtd, (size_t)n)) || (rc = b->alloc(&b->d_dt, (size_t)n)) ||
+      (rc = b->alloc(&b->d_lam, 2 * (size_t)n)) || (rc = b->alloc(&b->d_bad, (size_t)n)) ||
+      (rc = b->alloc(&b->d_st, (size_t)n)) || (rc = b->alloc(&b->d_ctl, 1)) ||
+      (rc = b->alloc(&b->d_iters, (size_t)kSolves * n)))
+    return cleanup(rc);
+  if (cudaMemcpy(b->d_rhs_work, rw.data(), sizeof(int4) * rw.size(), cudaMemcpyHostToDevice) ||
+      cudaMemcpy(b->d_cells, cb.data(), sizeof(int2) * cb.size(), cudaMemcpyHostToDevice) ||
+      cudaMemcpy(b->d_tiles, tl.data(), sizeof(int2) * tl.size(), cudaMemcpyHostToDevice) ||
+      cudaMemcpy(b->d_dtd, dd.data(), sizeof(DtBatchDesc) * n, cudaMemcpyHostToDevice))
+    return cleanup(bfail(SWM_ERR_CUDA, "table upload failed"));
+  if ((rc = batch_tables(b))) return cleanup(rc);
+  for (int c = 1; c <= kMaxBlock; c *= 2) {
+    b->jac_blocks[c] = jacobi_batch_grid_blocks(c, b->device, b->fast);
+    if (b->jac_blocks[c] < 1) return cleanup(bfail(SWM_ERR_CUDA, "Jacobi kernel cannot be resident"));
+  }
+  if (b->block != 1 && b->block != 2 && b->block != 4 && b->block != 8)
+    b->block = b->block < 2 ? 1 : (b->block < 4 ? 2 : (b->block < 8 ? 4 : 8));
+  b->h_dt.assign(n, 0.0);
+  b->h_iters.assign((size_t)kSolves * n, 0);
+  b->h_bad.assign(n, 0);
+  if (cudaDeviceSynchronize() != cudaSuccess) return cleanup(bfail(SWM_ERR_CUDA, "initialisation failed"));
+  *out = b;
+  return SWM_OK;
+}
+
 int swm_batch_set_planes(swm_batch_handle b, int i, const double* planes) {
-  if (!b || i < 0 || i >= (int)b->h.size()) return SWM_ERR_PARAM;
-  return swm_set_planes(b->h[i], planes);
+  if (!b || !planes || i < 0 || i >= b->n) return bfail(SWM_ERR_PARAM, "invalid argument");
+  BCK(cudaSetDevice(b->device));
+  const BProblem& q = b->pr[i];
+  BCK(cudaMemcpyAsync(q.h, planes, sizeof(double) * q.N, cudaMemcpyHostToDevice, b->stream));
+  BCK(cudaMemcpyAsync(q.hu, planes + q.N, sizeof(double) * q.N, cudaMemcpyHostToDevice, b->stream));
+  BCK(cudaMemcpyAsync(q.hv, planes + 2 * q.N, sizeof(double) * q.N, cudaMemcpyHostToDevice, b->stream));
+  BCK(cudaStreamSynchronize(b->stream));
+  b->have_state = true;
+  return SWM_OK;
 }
 
 int swm_batch_get_planes(swm_batch_handle b, int i, double* planes) {
-  if (!b || i < 0 || i >= (int)b->h.size()) return SWM_ERR_PARAM;
-  return swm_get_planes(b->h[i], planes);
+  if (!b || !planes || i < 0 || i >= b->n) return bfail(SWM_ERR_PARAM, "invalid argument");
+  BCK(cudaSetDevice(b->device));
+  const BProblem& q = b->pr[i];
+  BCK(cudaMemcpyAsync(planes, q.h, sizeof(double) * q.N, cudaMemcpyDeviceToHost, b->stream));
+  BCK(cudaMemcpyAsync(planes + q.N, q.hu, sizeof(double) * q.N, cudaMemcpyDeviceToHost, b->stream));
+  BCK(cudaMemcpyAsync(planes + 2 * q.N, q.hv, sizeof(double) * q.N, cudaMemcpyDeviceToHost, b->stream));
+  BCK(cudaStreamSynchronize(b->stream));
+  return SWM_OK;
 }
 
 int swm_batch_step(swm_batch_handle b, double* dt_out) {
-  if (!b) return SWM_ERR_PARAM;
-  int warn = 0;
-  for (size_t i = 0; i < b->h.size(); ++i) {
-    double dt;
-    int rc = swm_timestep(b->h[i], &dt);
-    if (rc < 0) return rc;
-    rc = swm_step(b->h[i], 0.0, dt);
-    if (rc < 0) return rc;
-    if (rc > 0) warn = rc;
-    if (dt_out) dt_out[i] = dt;
-  }
-  return warn;
+  if (!b) return bfail(SWM_ERR_PARAM, "null handle");
+  if (!b->have_state) return bfail(SWM_ERR_STATE, "no state set");
+  BCK(cudaSetDevice(b->device));
+  int rc;
+  if (b->autotune && (rc = batch_tune(b))) return rc;
+  if ((rc = batch_graph(b))) return rc;
+  BCK(cudaGraphLaunch(b->graph, b->stream));
+  JacBatchCtl ctl;
+  BCK(cudaMemcpyAsync(b->h_dt.data(), b->d_dt, sizeof(double) * b->n, cudaMemcpyDeviceToHost, b->stream));
+  BCK(cudaMemcpyAsync(b->h_iters.data(), b->d_iters, sizeof(int) * b->h_iters.size(),
+                      cudaMemcpyDeviceToHost, b->stream));
+  BCK(cudaMemcpyAsync(b->h_bad.data(), b->d_bad, sizeof(int) * b->n, cudaMemcpyDeviceToHost, b->stream));
+  BCK(cudaMemcpyAsync(&ctl, b->d_ctl, sizeof(JacBatchCtl), cudaMemcpyDeviceToHost, b->stream));
+  BCK(cudaStreamSynchronize(b->stream));
+  if (dt_out)
+    for (int i = 0; i < b->n; ++i) dt_out[i] = b->h_dt[i];
+  for (int v : b->h_iters) b->iters_total += v;
+  for (int v : b->h_bad)
+    if (v) return bfail(SWM_ERR_NAN, "non-finite or negative depth in an ensemble member");
+  if (ctl.status < 0) return bfail(SWM_ERR_WATCHDOG, "Jacobi grid barrier watchdog expired");
+  if (ctl.status == 1) return SWM_WARN_JACOBI_MAXITER;
+  return SWM_OK;
 }
 
 int swm_batch_cells(swm_batch_handle b, long long* cells) {
-  if (!b || !cells) return SWM_ERR_PARAM;
-  long long s = 0;
-  for (auto c : b->cells) s += c;
-  *cells = s;
+  if (!b || !cells) return bfail(SWM_ERR_PARAM, "invalid argument");
+  *cells = b->cells;
+  return SWM_OK;
+}
+
+int swm_batch_get_stats(swm_batch_handle b, int* jacobi_block, long long* iters_total,
+                        int* last_iters) {
+  if (!b) return bfail(SWM_ERR_PARAM, "null handle");
+  if (jacobi_block) *jacobi_block = b->block;
+  if (iters_total) *iters_total = b->iters_total;
+  if (last_iters)
+    for (size_t k = 0; k < b->h_iters.size(); ++k) last_iters[k] = b->h_iters[k];
+  return SWM_OK;
+}
+
+int swm_batch_get_stream(swm_batch_handle b, void** stream) {
+  if (!b || !stream) return bfail(SWM_ERR_PARAM, "invalid argument");
+  *stream = (void*)b->stream;
   return SWM_OK;
 }
 

@@ -229,10 +229,8 @@ __device__ __forceinline__ double patankar_weight(double h) {
 }
 
 template <bool FAST>
-__global__ void assemble_kernel(const AssembleArgs a, bool csr) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y;
-  if (i >= a.nx || j >= a.ny) return;
+__device__ __forceinline__ void assemble_cell(const AssembleArgs& a, bool csr, const int i,
+                                              const int j) {
   const int nx = a.nx, ny = a.ny;
   const size_t k = (size_t)j * nx + i;
   const double dt = *a.dt;
@@ -321,6 +319,41 @@ __global__ void assemble_kernel(const AssembleArgs a, bool csr) {
   if (a.rhs_out) a.rhs_out[k] = hp_read(a, 0, i, j);  // rhs = hp(1,.) (timediscretization.f90:887)
 }
 
+template <bool FAST>
+__global__ void assemble_kernel(const AssembleArgs a, bool csr) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y;
+  if (i >= a.nx || j >= a.ny) return;
+  assemble_cell<FAST>(a, csr, i, j);
+}
+
+// Ensembles: block b covers cells [cell0, cell0+128) of problem blk[b].x, with
+// cell0 = blk[b].y; descriptors staged in shared memory (stencil layout only).
+template <bool FAST>
+__global__ void __launch_bounds__(128)
+    assemble_batch_kernel(const AssembleArgs* __restrict__ descs, const int2* __restrict__ blk) {
+  static_assert(sizeof(AssembleArgs) % 8 == 0 && sizeof(AssembleArgs) / 8 <= 128, "copy");
+  __shared__ __align__(16) AssembleArgs sa;
+  const int2 w = blk[blockIdx.x];
+  if (threadIdx.x < sizeof(AssembleArgs) / 8)
+    reinterpret_cast<unsigned long long*>(&sa)[threadIdx.x] =
+        reinterpret_cast<const unsigned long long*>(&descs[w.x])[threadIdx.x];
+  __syncthreads();
+  const int c = w.y + threadIdx.x;
+  if (c >= sa.nx * sa.ny) return;
+  assemble_cell<FAST>(sa, false, c % sa.nx, c / sa.nx);
+}
+
+cudaError_t launch_assemble_batch(const AssembleArgs* descs, const int2* blk, int nblk, bool fast,
+                                  cudaStream_t s) {
+  if (nblk < 1) return cudaSuccess;
+  if (fast)
+    assemble_batch_kernel<true><<<nblk, 128, 0, s>>>(descs, blk);
+  else
+    assemble_batch_kernel<false><<<nblk, 128, 0, s>>>(descs, blk);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_assemble(const AssembleArgs& a, bool csr, cudaStream_t s) {
   dim3 blk(128), grd((a.nx + 127) / 128, a.ny);
   if (a.fast && !csr)
@@ -337,7 +370,9 @@ cudaError_t launch_assemble(const AssembleArgs& a, bool csr, cudaStream_t s) {
 // grid barrier; the stop decision is taken identically by every CTA from the
 // integer residual sums.
 // ---------------------------------------------------------------------------
-__device__ bool grid_barrier(JacobiCtl* ctl, long long spin_limit, int* s_ok) {
+// C: JacobiCtl or JacBatchCtl (bar_count, bar_gen, status).
+template <typename C>
+__device__ bool grid_barrier(C* ctl, long long spin_limit, int* s_ok) {
   __syncthreads();
   if (threadIdx.x == 0) {
     volatile unsigned int* vgen = &ctl->bar_gen;
@@ -410,9 +445,9 @@ __device__ __forceinline__ int wrap_near(int g, int n) {
 // JBX x JBY block of cells plus a TB-cell halo in shared memory; sweep t updates
 // the region shrunk by t, so after Tp sweeps the tile interior holds x^{k+Tp},
 // bit-identical to Tp global sweeps.  Warps own rows, lanes own columns.
-template <int TB, bool RECIP>
-__device__ void stencil_pass(const JacobiArgs& a, const double* xin, double* xout, int Tp,
-                             bool first, Acc& acc, double* sm) {
+template <int TB, bool RECIP, bool ONE_TILE>
+__device__ void stencil_tiles(const JacobiArgs& a, const double* xin, double* xout, int Tp,
+                              bool first, Acc& acc, double* sm, int tile_first) {
   using G = JTile<TB>;
   constexpr int HX = G::HX, HY = G::HY, HN = G::HN, NW = JNT / 32;
   double* sS = sm;
@@ -429,7 +464,10 @@ __device__ void stencil_pass(const JacobiArgs& a, const double* xin, double* xou
   // 16-byte pairs need an even first column (i0 - TB) and an even row pitch
   const bool pairs = (TB % 2 == 0) && !small && (nx % 2 == 0);
   const int tx = (nx + JBX - 1) / JBX, ty = (ny + JBY - 1) / JBY;
-  for (int tile = blockIdx.x; tile < tx * ty; tile += gridDim.x) {
+  // ONE_TILE: exactly tile `tile_first` (ensembles); else every CTA-strided tile
+  const int t_end = ONE_TILE ? tile_first + 1 : tx * ty;
+  const int t_step = ONE_TILE ? 1 : gridDim.x;
+  for (int tile = tile_first; tile < t_end; tile += t_step) {
     const int i0 = (tile % tx) * JBX, j0 = (tile / tx) * JBY;
     if (pairs) {
       // even nx, no multiple wrap: 16-byte pairs (gi even) never straddle the seam
@@ -572,7 +610,7 @@ __global__ void __launch_bounds__(JNT, 2) jacobi_kernel(const JacobiArgs a) {
     if (CSR)
       csr_pass(a, xin, xout, first, acc);
     else
-      stencil_pass<TB, RECIP>(a, xin, xout, Tp, first, acc, jsm);
+      stencil_tiles<TB, RECIP, false>(a, xin, xout, Tp, first, acc, jsm, blockIdx.x);
     acc_reduce<TB>(acc, s_acc);
     __syncthreads();
     const int slot = p % kResSlots;
@@ -616,7 +654,7 @@ __global__ void __launch_bounds__(JNT, 2) jacobi_kernel(const JacobiArgs a) {
         for (int q = threadIdx.x; q < (kMaxBlock + 1) * 3; q += blockDim.x)
           (&s_acc[0][0])[q] = 0ull;
         __syncthreads();
-        stencil_pass<TB, RECIP>(a, xin, xout, stop, false, acc, jsm);
+        stencil_tiles<TB, RECIP, false>(a, xin, xout, stop, false, acc, jsm, blockIdx.x);
         acc_reduce<TB>(acc, s_acc);
         if (!grid_barrier(ctl, a.spin_limit, &s_ok)) return;
         if (blockIdx.x == 0) {
@@ -723,6 +761,274 @@ cudaError_t launch_jacobi(const JacobiArgs& a, bool csr, int grid_blocks, cudaSt
   cfg.numAttrs = 1;
   void* args[] = {const_cast<JacobiArgs*>(&a)};
   return cudaLaunchKernelExC(&cfg, fn, args);
+}
+
+// ---------------------------------------------------------------------------
+// Ensembles: one cooperative launch solves the Patankar systems of every problem.
+// Each pass visits the tiles of all still-active problems; residual limbs are
+// flushed per tile into that problem's accumulators; after a grid barrier CTA 0
+// applies the single-problem stop rule to every problem (stop, redo the pass with
+// fewer sweeps, or continue), and a second barrier publishes the decisions.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int xout_id(int cur) { return cur == 1 ? 2 : 1; }
+
+// CTA 0: the stop rule of jacobi_iteration.f90:71-81 for every active problem.
+__device__ void batch_decide(const JacobiBatchArgs& a, int blk, int* s_cnt) {
+  if (threadIdx.x == 0) *s_cnt = 0;
+  __syncthreads();
+  int active = 0;
+  for (int p = threadIdx.x; p < a.nprob; p += blockDim.x) {
+    JacBatchState* S = &a.st[p];
+    if (!__ldcg(&S->active)) continue;
+    const JacobiArgs& d = a.descs[p];
+    int k = __ldcg(&S->k), Tp = __ldcg(&S->Tp), cur = __ldcg(&S->cur);
+    const int first = __ldcg(&S->first), rollback = __ldcg(&S->rollback);
+    int act = 1;
+    if (rollback) {  // the redone pass delivered x^{final_k}
+      act = 0;
+      S->result = xout_id(cur);
+    } else {
+      int stop = -1;
+      if (first && limbs_le(__ldcg(&S->acc[0][0]), __ldcg(&S->acc[0][1]),
+                            __ldcg(&S->acc[0][2]), d.thresh)) {
+        stop = 0;
+      } else {
+        for (int t = 1; t <= Tp; ++t)
+          if (limbs_le(__ldcg(&S->acc[t][0]), __ldcg(&S->acc[t][1]), __ldcg(&S->acc[t][2]),
+                       d.thresh)) {
+            stop = t;
+            break;
+          }
+      }
+      S->first = 0;
+      if (stop == 0) {
+        act = 0;
+        S->result = 0;
+        S->final_k = 0;
+      } else if (stop > 0) {
+        S->final_k = k + stop;
+        if (stop < Tp) {
+          S->rollback = 1;
+          S->Tp = stop;
+        } else {
+          act = 0;
+          S->result = xout_id(cur);
+        }
+      } else {
+        k += Tp;
+        S->k = k;
+        if (k >= d.maxiter) {
+          act = 0;
+          S->maxhit = 1;
+          S->final_k = k;
+          S->result = xout_id(cur);
+        } else {
+          S->cur = xout_id(cur);
+          S->Tp = (d.maxiter - k < blk) ? d.maxiter - k : blk;
+        }
+      }
+    }
+    S->active = act;
+    for (int q = 0; q < (kMaxBlock + 1) * 3; ++q) (&S->acc[0][0])[q] = 0ull;
+    active += act;
+  }
+  if (active) atomicAdd(s_cnt, active);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    a.ctl->n_active = *s_cnt;
+    __threadfence();
+  }
+}
+
+template <int TB, bool RECIP>
+__global__ void __launch_bounds__(JNT, 2) jacobi_batch_kernel(const JacobiBatchArgs a) {
+  extern __shared__ __align__(16) double jsm[];
+  __shared__ unsigned long long s_acc[kMaxBlock + 1][3];
+  __shared__ __align__(16) JacobiArgs sd;
+  __shared__ int s_ok, s_cnt, s_p, s_active, s_Tp, s_first, s_cur;
+  static_assert(sizeof(JacobiArgs) % 8 == 0 && sizeof(JacobiArgs) / 8 <= JNT, "descriptor copy");
+  const int blk = a.block < 1 ? 1 : (a.block > TB ? TB : a.block);
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < a.nprob; p += gridDim.x * blockDim.x) {
+    JacBatchState* S = &a.st[p];
+    const int mi = a.descs[p].maxiter;
+    S->active = 1;
+    S->k = 0;
+    S->Tp = (mi < blk) ? mi : blk;
+    S->rollback = 0;
+    S->first = 1;
+    S->cur = 0;
+    S->result = 0;
+    S->final_k = 0;
+    S->maxhit = 0;
+    for (int q = 0; q < (kMaxBlock + 1) * 3; ++q) (&S->acc[0][0])[q] = 0ull;
+  }
+  if (!grid_barrier(a.ctl, a.spin_limit, &s_ok)) return;
+  Acc acc;
+#pragma unroll
+  for (int t = 0; t <= kMaxBlock; ++t)
+#pragma unroll
+    for (int l = 0; l < 3; ++l) acc.v[t][l] = 0ull;
+  int loaded = -1;
+  for (;;) {
+    for (int w = blockIdx.x; w < a.ntiles; w += gridDim.x) {
+      const int2 t = a.tiles[w];
+      if (threadIdx.x == 0) {
+        const JacBatchState* S = &a.st[t.x];
+        s_p = t.x;
+        s_active = __ldcg(&S->active);
+        s_Tp = __ldcg(&S->Tp);
+        s_first = __ldcg(&S->first);
+        s_cur = __ldcg(&S->cur);
+      }
+      if (t.x != loaded) {  // stage this problem's descriptor
+        if (threadIdx.x < sizeof(JacobiArgs) / 8)
+          reinterpret_cast<unsigned long long*>(&sd)[threadIdx.x] =
+              reinterpret_cast<const unsigned long long*>(&a.descs[t.x])[threadIdx.x];
+        loaded = t.x;
+      }
+      if (threadIdx.x < (kMaxBlock + 1) * 3) (&s_acc[0][0])[threadIdx.x] = 0ull;
+      __syncthreads();
+      if (s_active) {
+        const double* xin = s_cur == 0 ? sd.b : (s_cur == 1 ? sd.xa : sd.xb);
+        double* xout = s_cur == 1 ? sd.xb : sd.xa;
+        stencil_tiles<TB, RECIP, true>(sd, xin, xout, s_Tp, s_first != 0, acc, jsm, t.y);
+        acc_reduce<TB>(acc, s_acc);
+        __syncthreads();
+        if (threadIdx.x < (TB + 1) * 3) {
+          const unsigned long long v = (&s_acc[0][0])[threadIdx.x];
+          if (v) atomicAdd(&(&a.st[s_p].acc[0][0])[threadIdx.x], v);
+        }
+      }
+      __syncthreads();
+    }
+    if (!grid_barrier(a.ctl, a.spin_limit, &s_ok)) return;
+    if (blockIdx.x == 0) batch_decide(a, blk, &s_cnt);
+    if (!grid_barrier(a.ctl, a.spin_limit, &s_ok)) return;
+    if (threadIdx.x == 0) s_cnt = __ldcg(&a.ctl->n_active);
+    __syncthreads();
+    if (s_cnt == 0) break;
+  }
+  // deliver every problem's final iterate (haVec) to its destination
+  for (int p = 0; p < a.nprob; ++p) {
+    const JacobiArgs& d = a.descs[p];
+    const int res = __ldcg(&a.st[p].result);
+    const double* src = res == 1 ? d.xa : d.xb;
+    const int n = d.nx * d.ny;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x)
+      d.out[q] = res == 0 ? 0. : __ldcg(&src[q]);
+  }
+  if (blockIdx.x == 0) {
+    for (int p = threadIdx.x; p < a.nprob; p += blockDim.x) {
+      a.iters[p] = __ldcg(&a.st[p].final_k);
+      if (__ldcg(&a.st[p].maxhit)) atomicMax(&a.ctl->status, 1);
+    }
+  }
+}
+
+template <bool RECIP>
+static const void* pick_batch(int block, size_t* smem) {
+  if (block <= 1) {
+    *smem = JTile<1>::bytes;
+    return reinterpret_cast<const void*>(&jacobi_batch_kernel<1, RECIP>);
+  }
+  if (block <= 2) {
+    *smem = JTile<2>::bytes;
+    return reinterpret_cast<const void*>(&jacobi_batch_kernel<2, RECIP>);
+  }
+  if (block <= 4) {
+    *smem = JTile<4>::bytes;
+    return reinterpret_cast<const void*>(&jacobi_batch_kernel<4, RECIP>);
+  }
+  *smem = JTile<8>::bytes;
+  return reinterpret_cast<const void*>(&jacobi_batch_kernel<8, RECIP>);
+}
+
+int jacobi_batch_grid_blocks(int block, int device, bool recip) {
+  size_t smem = 0;
+  const void* fn = recip ? pick_batch<true>(block, &smem) : pick_batch<false>(block, &smem);
+  if (smem > 48 * 1024)
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int per_sm = 0, sms = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, JNT, smem) != cudaSuccess)
+    return -1;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  return per_sm < 1 ? -1 : per_sm * sms;
+}
+
+cudaError_t launch_jacobi_batch(const JacobiBatchArgs& a, int grid_blocks, bool recip,
+                                cudaStream_t s) {
+  size_t smem = 0;
+  const void* fn = recip ? pick_batch<true>(a.block, &smem) : pick_batch<false>(a.block, &smem);
+  int blocks = grid_blocks < a.ntiles ? grid_blocks : a.ntiles;
+  if (blocks < 1) blocks = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(blocks);
+  cfg.blockDim = dim3(JNT);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  void* args[] = {const_cast<JacobiBatchArgs*>(&a)};
+  return cudaLaunchKernelExC(&cfg, fn, args);
+}
+
+// Batched TimeStep: block b covers 128 cells of problem blk[b].x from blk[b].y.
+__global__ void __launch_bounds__(128)
+    dt_batch_kernel(const DtBatchDesc* __restrict__ d, const int2* __restrict__ blk,
+                    unsigned long long* lam, int* bad) {
+  const int2 w = blk[blockIdx.x];
+  const DtBatchDesc& q = d[w.x];
+  const int c = w.y + threadIdx.x;
+  double lx = 0.0, ly = 0.0;
+  int b = 0;
+  if (c < q.nx * q.ny) {
+    double h = q.h[c], hu = q.hu[c], hv = q.hv[c], u, v;
+    if (!(h >= 0.0) || !isfinite(h) || !isfinite(hu) || !isfinite(hv)) b = 1;
+    cons_to_prim(h, hu, hv, u, v);
+    double cc = sqrt(q.g * h);
+    lx = fabs(u + cc);
+    ly = fabs(v + cc);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    lx = dmax(lx, __shfl_down_sync(0xffffffffu, lx, o));
+    ly = dmax(ly, __shfl_down_sync(0xffffffffu, ly, o));
+  }
+  b = __any_sync(0xffffffffu, b);
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(&lam[2 * w.x], (unsigned long long)__double_as_longlong(lx));
+    atomicMax(&lam[2 * w.x + 1], (unsigned long long)__double_as_longlong(ly));
+    if (b) atomicOr(&bad[w.x], 1);
+  }
+}
+
+// dt = CFL * min(HUGE, dx/LambdaMaxX, dy/LambdaMaxY), floored (equation.f90:818-834)
+__global__ void dt_finalize_kernel(const DtBatchDesc* d, int nprob, const unsigned long long* lam,
+                                   double* dt) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= nprob) return;
+  const double LX = __longlong_as_double((long long)lam[2 * p]);
+  const double LY = __longlong_as_double((long long)lam[2 * p + 1]);
+  double ts = 1.7976931348623157e308;
+  const double a1 = d[p].dx / LX, b1 = d[p].dy / LY;
+  if (a1 < ts) ts = a1;
+  if (b1 < ts) ts = b1;
+  ts = d[p].cfl * ts;
+  if (ts < 1.0e-30) ts = 1.0e-30;
+  dt[p] = ts;
+}
+
+cudaError_t launch_dt_batch(const DtBatchDesc* d, const int2* blk, int nblk, int nprob,
+                            unsigned long long* lam, int* bad, double* dt, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(lam, 0, sizeof(unsigned long long) * 2 * nprob, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(bad, 0, sizeof(int) * nprob, s);
+  if (e != cudaSuccess) return e;
+  dt_batch_kernel<<<nblk, 128, 0, s>>>(d, blk, lam, bad);
+  dt_finalize_kernel<<<(nprob + 127) / 128, 128, 0, s>>>(d, nprob, lam, dt);
+  return cudaGetLastError();
 }
 
 }  // namespace swm

@@ -93,7 +93,56 @@ struct DtArgs {
   int* bad;                 // non-finite or negative depth seen
 };
 
+// ---- ensembles: one launch covers every problem ----
+// Jacobi state of one problem during a batched solve (global memory).
+struct JacBatchState {
+  int active;    // still iterating
+  int k;         // sweeps done
+  int Tp;        // sweeps of the coming pass
+  int rollback;  // the coming pass redoes the last one with Tp sweeps
+  int first;     // the coming pass is the first (initial residual checked)
+  int cur;       // buffer holding x^k: 0 = b, 1 = xa, 2 = xb
+  int result;    // final iterate: 0 = zero vector, 1 = xa, 2 = xb
+  int final_k;
+  int maxhit;
+  int pad;
+  unsigned long long acc[kMaxBlock + 1][3];
+};
+struct JacBatchCtl {
+  unsigned int bar_count, bar_gen;
+  int n_active;
+  int status;  // 0 ok, 1 some problem hit maxIter, -4 watchdog
+};
+struct JacobiBatchArgs {
+  const JacobiArgs* descs;  // per problem: nx, ny, b, stencil planes, xa, xb, out, thresh, maxiter
+  const int2* tiles;        // (problem, tile index) of every tile of every problem
+  int ntiles, nprob;
+  JacBatchState* st;        // [nprob]
+  JacBatchCtl* ctl;
+  int* iters;               // [nprob] sweeps of this solve
+  int block;
+  long long spin_limit;
+};
+struct DtBatchDesc {
+  int nx, ny;
+  double g, cfl, dx, dy;
+  const double* h;
+  const double* hu;
+  const double* hv;
+};
+
 // Host launchers (swm_kernels.cu, swm_rhs_*.cu)
+cudaError_t launch_rhs_batch_fast(int mode, const RhsArgs* descs, const int4* work, int nwork,
+                                  cudaStream_t s);
+cudaError_t launch_rhs_batch_exact(const RhsArgs* descs, const int4* work, int nwork,
+                                   cudaStream_t s);
+cudaError_t launch_assemble_batch(const AssembleArgs* descs, const int2* blk, int nblk, bool fast,
+                                  cudaStream_t s);
+cudaError_t launch_jacobi_batch(const JacobiBatchArgs& a, int grid_blocks, bool recip,
+                                cudaStream_t s);
+int jacobi_batch_grid_blocks(int block, int device, bool recip);
+cudaError_t launch_dt_batch(const DtBatchDesc* d, const int2* blk, int nblk, int nprob,
+                            unsigned long long* lam, int* bad, double* dt, cudaStream_t s);
 cudaError_t launch_rhs_fast(int mode, const RhsArgs& a, cudaStream_t s);
 cudaError_t launch_rhs_exact(const RhsArgs& a, cudaStream_t s);
 size_t rhs_smem_bytes(int mode);

@@ -76,9 +76,9 @@ struct RhsSmem {
 namespace swm {
 namespace SWM_RHS_NS {
 
-// MODE: 0 FP64 (EXACT per translation unit), 1 SPLIT.
+// MODE: 0 FP64 (EXACT per translation unit), 1 SPLIT.  One CTA, tile origin (i0, j0).
 template <int MODE>
-__global__ void __launch_bounds__(RHS_NT, 2) rhs_kernel(const RhsArgs a) {
+__device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const int j0) {
   using T = typename std::conditional<MODE == 1, float, double>::type;
   constexpr bool EX = (MODE == 0) && SWM_EXACT;
   constexpr int TX = RHS_TX, TY = RHS_TY, NT = RHS_NT;
@@ -93,7 +93,6 @@ __global__ void __launch_bounds__(RHS_NT, 2) rhs_kernel(const RhsArgs a) {
 
   const Grid& gr = a.gr;
   const int nx = gr.nx, ny = gr.ny;
-  const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
   const int tid = threadIdx.x;
 
   // ---- load the haloed tile, V = ConsToPrim(U) (equation.f90:778-782) ----
@@ -404,6 +403,26 @@ __global__ void __launch_bounds__(RHS_NT, 2) rhs_kernel(const RhsArgs a) {
     }
   }
 #undef SV
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(RHS_NT, 2) rhs_kernel(const RhsArgs a) {
+  rhs_tile<MODE>(a, blockIdx.x * RHS_TX, blockIdx.y * RHS_TY);
+}
+
+// Ensembles: CTA b computes tile (work[b].y, work[b].z) of problem work[b].x, whose
+// descriptor is staged in shared memory; one launch covers every problem's tiles.
+template <int MODE>
+__global__ void __launch_bounds__(RHS_NT, 2)
+    rhs_batch_kernel(const RhsArgs* __restrict__ descs, const int4* __restrict__ work) {
+  static_assert(sizeof(RhsArgs) % 8 == 0 && sizeof(RhsArgs) / 8 <= RHS_NT, "descriptor copy");
+  __shared__ __align__(16) RhsArgs sa;
+  const int4 w = work[blockIdx.x];
+  if (threadIdx.x < sizeof(RhsArgs) / 8)
+    reinterpret_cast<unsigned long long*>(&sa)[threadIdx.x] =
+        reinterpret_cast<const unsigned long long*>(&descs[w.x])[threadIdx.x];
+  __syncthreads();
+  rhs_tile<MODE>(sa, w.y, w.z);
 }
 
 }  // namespace SWM_RHS_NS

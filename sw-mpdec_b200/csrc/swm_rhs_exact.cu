@@ -21,4 +21,14 @@ cudaError_t launch_rhs_exact(const RhsArgs& a, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+cudaError_t launch_rhs_batch_exact(const RhsArgs* descs, const int4* work, int nwork,
+                                   cudaStream_t s) {
+  if (nwork < 1) return cudaSuccess;
+  size_t sm = RhsSmem<double>::bytes;
+  cudaFuncSetAttribute(rhs_exact::rhs_batch_kernel<0>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  rhs_exact::rhs_batch_kernel<0><<<nwork, RHS_NT, sm, s>>>(descs, work);
+  return cudaGetLastError();
+}
+
 }  // namespace swm

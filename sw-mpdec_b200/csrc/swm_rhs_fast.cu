@@ -34,4 +34,21 @@ cudaError_t launch_rhs_fast(int mode, const RhsArgs& a, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+cudaError_t launch_rhs_batch_fast(int mode, const RhsArgs* descs, const int4* work, int nwork,
+                                  cudaStream_t s) {
+  if (nwork < 1) return cudaSuccess;
+  if (mode == 1) {
+    size_t sm = RhsSmem<float>::bytes;
+    cudaFuncSetAttribute(rhs_fast::rhs_batch_kernel<1>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    rhs_fast::rhs_batch_kernel<1><<<nwork, RHS_NT, sm, s>>>(descs, work);
+  } else {
+    size_t sm = RhsSmem<double>::bytes;
+    cudaFuncSetAttribute(rhs_fast::rhs_batch_kernel<0>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    rhs_fast::rhs_batch_kernel<0><<<nwork, RHS_NT, sm, s>>>(descs, work);
+  }
+  return cudaGetLastError();
+}
+
 }  // namespace swm

@@ -27,7 +27,7 @@ EXPORTS = [
     "swm_run", "swm_get_stats", "swm_state_summary", "swm_last_error", "swm_strerror",
     "swm_get_stream", "swm_profile_step", "swm_debug_rhs", "swm_debug_jacobi", "swm_batch_create", "swm_batch_destroy",
     "swm_batch_set_planes", "swm_batch_get_planes", "swm_batch_step", "swm_batch_cells",
-    "swm_jacobi_noalloc",
+    "swm_jacobi_noalloc", "swm_batch_get_stats", "swm_batch_get_stream",
 ]
 
 
@@ -102,6 +102,9 @@ def load():
     lib.swm_batch_get_planes.argtypes = [vp, ctypes.c_int, dp]
     lib.swm_batch_step.argtypes = [vp, dp]
     lib.swm_batch_cells.argtypes = [vp, P(ctypes.c_longlong)]
+    lib.swm_batch_get_stats.argtypes = [vp, P(ctypes.c_int), P(ctypes.c_longlong),
+                                        P(ctypes.c_int)]
+    lib.swm_batch_get_stream.argtypes = [vp, P(vp)]
     lib.swm_jacobi_noalloc.argtypes = ([ctypes.c_int, ctypes.c_int] + [vp] * 7 +
                                        [ctypes.c_int, ctypes.c_double, ctypes.c_int,
                                         P(ctypes.c_int), vp])
@@ -301,3 +304,16 @@ class Batch:
         c = ctypes.c_longlong()
         _check(self.lib.swm_batch_cells(self.h, ctypes.byref(c)))
         return c.value
+
+    def stream(self):
+        p = ctypes.c_void_p()
+        _check(self.lib.swm_batch_get_stream(self.h, ctypes.byref(p)))
+        return p.value or 0
+
+    def stats(self):
+        """(sweeps per Jacobi pass, total sweeps, last step's sweeps [13][n])."""
+        blk, tot = ctypes.c_int(), ctypes.c_longlong()
+        last = np.zeros(13 * len(self.params), dtype=np.int32)
+        _check(self.lib.swm_batch_get_stats(self.h, ctypes.byref(blk), ctypes.byref(tot),
+                                            last.ctypes.data_as(ctypes.POINTER(ctypes.c_int))))
+        return blk.value, tot.value, last.reshape(13, len(self.params))
