@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "../../include/swm.h"
+#include "swm_host.h"
 #include "swm_kernels.cuh"
 
 using namespace swm;
@@ -60,50 +61,9 @@ struct BProblem {
   double* fym[4] = {};
   double *cS = nullptr, *cW = nullptr, *cE = nullptr, *cN = nullptr, *cD = nullptr;
   double *xa = nullptr, *xb = nullptr;
-  double *gex = nullptr, *gey = nullptr, *bgrad = nullptr;
+  double *src_col = nullptr, *src_row = nullptr, *bgrad = nullptr;
   double* save[3] = {};  // state copy used while tuning
 };
-
-void quad(double qn[4], double qw[4]) {  // mesh.f90:127-129
-  qw[0] = (18. - sqrt(30.)) / 72.;
-  qw[1] = (18. + sqrt(30.)) / 72.;
-  qw[2] = (18. + sqrt(30.)) / 72.;
-  qw[3] = (18. - sqrt(30.)) / 72.;
-  qn[0] = -(0.5 * sqrt(3. / 7. + 2. / 7. * sqrt(6. / 5.)));
-  qn[1] = -(0.5 * sqrt(3. / 7. - 2. / 7. * sqrt(6. / 5.)));
-  qn[2] = 0.5 * sqrt(3. / 7. - 2. / 7. * sqrt(6. / 5.));
-  qn[3] = 0.5 * sqrt(3. / 7. + 2. / 7. * sqrt(6. / 5.));
-}
-
-double gpx(double x0, double h, int c, double q) {
-  double node = x0 + ((double)c) * h;
-  double bary = node + 0.5 * h;
-  return bary + q * h;
-}
-
-// Bathymetry_X/_Y (equation.f90:451-509) and the Gaussian case, on the host.
-void bgrad_host(const swm_params& p, double x, double y, double* bx, double* by) {
-  const double PI = acos(-1.0);
-  *bx = 0.;
-  *by = 0.;
-  if (p.bathy_flag == SWM_BATHY_SINCOS) {
-    *bx = 0.1 * 2. * PI * cos(2. * PI * x) * cos(2. * PI * y);
-    *by = -(0.1 * 2. * PI * sin(2. * PI * x) * sin(2. * PI * y));
-  } else if (p.bathy_flag == SWM_BATHY_BUMP) {
-    double r2 = x * x + y * y;
-    if (r2 < 1) {
-      double d = 1.0 - r2, e = exp(1.0 - 1.0 / d);
-      *bx = -(2.0 * x / (d * d) * e);
-      *by = -(2.0 * y / (d * d) * e);
-    }
-  } else if (p.bathy_flag == SWM_BATHY_GAUSS) {
-    double dxv = x - p.bathy_par[2], dyv = y - p.bathy_par[4];
-    double e = exp(-(p.bathy_par[1] * (dxv * dxv) + p.bathy_par[3] * (dyv * dyv)));
-    double B = p.bathy_par[0] * e;
-    *bx = (-2.0 * p.bathy_par[1] * dxv) * B;
-    *by = (-2.0 * p.bathy_par[3] * dyv) * B;
-  }
-}
 
 }  // namespace
 
@@ -200,35 +160,17 @@ static int batch_alloc_problem(swm_batch* b, BProblem& q) {
 #undef BA
   if (rc) return rc;
   const Grid& gr = q.gr;
-  if (q.p.bathy_flag == SWM_BATHY_GAUSS && q.p.precision != SWM_PREC_FP64) {
-    if ((rc = b->alloc(&q.gex, 4 * (size_t)q.nx)) || (rc = b->alloc(&q.gey, 4 * (size_t)q.ny)))
+  if (separable_source(q.p)) {
+    std::vector<double> col, row;
+    host_source_factors(q.p, gr, col, row);
+    if ((rc = b->alloc(&q.src_col, col.size())) || (rc = b->alloc(&q.src_row, row.size())))
       return rc;
-    std::vector<double> ex(4 * q.nx), ey(4 * q.ny);
-    for (int i = 0; i < q.nx; ++i)
-      for (int k = 0; k < 4; ++k) {
-        double d = gpx(gr.x0, gr.dx, i, gr.qn[k]) - gr.bp[2];
-        ex[4 * i + k] = exp(-(gr.bp[1] * (d * d)));
-      }
-    for (int j = 0; j < q.ny; ++j)
-      for (int k = 0; k < 4; ++k) {
-        double d = gpx(gr.y0, gr.dy, j, gr.qn[k]) - gr.bp[4];
-        ey[4 * j + k] = exp(-(gr.bp[3] * (d * d)));
-      }
-    BCK(cudaMemcpy(q.gex, ex.data(), sizeof(double) * ex.size(), cudaMemcpyHostToDevice));
-    BCK(cudaMemcpy(q.gey, ey.data(), sizeof(double) * ey.size(), cudaMemcpyHostToDevice));
-  } else if (q.p.bathy_flag > 0) {
-    if ((rc = b->alloc(&q.bgrad, 32 * N))) return rc;
-    std::vector<double> tab(32 * N);
-    for (int a = 0; a < 4; ++a)
-      for (int c = 0; c < 4; ++c)
-        for (int j = 0; j < q.ny; ++j)
-          for (int i = 0; i < q.nx; ++i) {
-            double bx, by;
-            bgrad_host(q.p, gpx(gr.x0, gr.dx, i, gr.qn[a]), gpx(gr.y0, gr.dy, j, gr.qn[c]), &bx,
-                       &by);
-            tab[((a * 4 + c) * 2 + 0) * N + (size_t)j * q.nx + i] = bx;
-            tab[((a * 4 + c) * 2 + 1) * N + (size_t)j * q.nx + i] = by;
-          }
+    BCK(cudaMemcpy(q.src_col, col.data(), sizeof(double) * col.size(), cudaMemcpyHostToDevice));
+    BCK(cudaMemcpy(q.src_row, row.data(), sizeof(double) * row.size(), cudaMemcpyHostToDevice));
+  } else if (full_source_table(q.p)) {
+    std::vector<double> tab;
+    host_bgrad_table(q.p, gr, tab);
+    if ((rc = b->alloc(&q.bgrad, tab.size()))) return rc;
     BCK(cudaMemcpy(q.bgrad, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice));
   }
   return SWM_OK;
@@ -246,8 +188,8 @@ static RhsArgs batch_rhs_desc(const BProblem& q, const double* h, const double* 
   a.ut_hv = q.fv[slot];
   a.fxm = q.fxm[slot];
   a.fym = q.fym[slot];
-  a.gauss_ex = q.gex;
-  a.gauss_ey = q.gey;
+  a.src_col = q.src_col;
+  a.src_row = q.src_row;
   a.bgrad = q.bgrad;
   return a;
 }
@@ -481,19 +423,8 @@ int swm_batch_create(int n, const swm_params* p, swm_batch_handle* out) {
     q.nx = p[i].nx;
     q.ny = p[i].ny;
     q.N = (size_t)q.nx * q.ny;
-    Grid& gr = q.gr;
-    gr.nx = q.nx;
-    gr.ny = q.ny;
-    gr.x0 = p[i].x0[0];
-    gr.y0 = p[i].x0[1];
-    gr.dx = fabs(fabs(p[i].x1[0] - p[i].x0[0])) / ((double)q.nx);
-    gr.dy = fabs(fabs(p[i].x1[1] - p[i].x0[1])) / ((double)q.ny);
-    gr.g = p[i].g;
-    gr.bathy = p[i].bathy_flag;
-    for (int k = 0; k < 5; ++k) gr.bp[k] = p[i].bathy_par[k];
-    quad(gr.qn, gr.qw);
-    for (int a = 0; a < 4; ++a)
-      for (int c = 0; c < 4; ++c) gr.wgp[a][c] = gr.qw[a] * gr.qw[c];
+    q.gr = host_grid(p[i]);
+    const Grid& gr = q.gr;
     if ((rc = batch_alloc_problem(b, q))) return cleanup(rc);
     for (int ty = 0; ty < (q.ny + RHS_TY - 1) / RHS_TY; ++ty)
       for (int tx = 0; tx < (q.nx + RHS_TX - 1) / RHS_TX; ++tx)

@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "../../include/swm.h"
+#include "swm_host.h"
 #include "swm_kernels.cuh"
 
 using namespace swm;
@@ -76,9 +77,10 @@ struct swm_solver {
   // well-balanced reference
   double *fxwb = nullptr, *fywb = nullptr, *swb = nullptr;
   bool have_wb = false;
-  // bathymetry factor tables (Gaussian)
-  double *gex = nullptr, *gey = nullptr;
-  double* bgrad = nullptr;  // [4][4][2][N] b_x, b_y at interior Gauss points
+  // bathymetry source tables: separable factors [nx][2][4], [ny][2][4] or the full
+  // gradient [4][4][2][N] at the interior Gauss points
+  double *src_col = nullptr, *src_row = nullptr;
+  double* bgrad = nullptr;
   // scalars
   double* dt_dev = nullptr;
   unsigned long long* lam = nullptr;
@@ -137,52 +139,6 @@ static int valid_params(const swm_params* p) {
   return SWM_OK;
 }
 
-static void quadrature(double qn[4], double qw[4]) {
-  // mesh.f90:127-129
-  qw[0] = (18. - sqrt(30.)) / 72.;
-  qw[1] = (18. + sqrt(30.)) / 72.;
-  qw[2] = (18. + sqrt(30.)) / 72.;
-  qw[3] = (18. - sqrt(30.)) / 72.;
-  qn[0] = -(0.5 * sqrt(3. / 7. + 2. / 7. * sqrt(6. / 5.)));
-  qn[1] = -(0.5 * sqrt(3. / 7. - 2. / 7. * sqrt(6. / 5.)));
-  qn[2] = 0.5 * sqrt(3. / 7. - 2. / 7. * sqrt(6. / 5.));
-  qn[3] = 0.5 * sqrt(3. / 7. + 2. / 7. * sqrt(6. / 5.));
-}
-
-static double host_gp(double x0, double h, int c, double q) {
-  double node = x0 + ((double)c) * h;
-  double bary = node + 0.5 * h;
-  return bary + q * h;
-}
-
-// Bathymetry_X / Bathymetry_Y (equation.f90:451-509) and the Gaussian case, evaluated
-// on the host (this translation unit is built without FP contraction).
-static void host_bathy_grad(const swm_params& p, double x, double y, double* bx, double* by) {
-  const double PI = acos(-1.0);
-  *bx = 0.;
-  *by = 0.;
-  if (p.bathy_flag == SWM_BATHY_SINCOS) {
-    *bx = 0.1 * 2. * PI * cos(2. * PI * x) * cos(2. * PI * y);
-    *by = -(0.1 * 2. * PI * sin(2. * PI * x) * sin(2. * PI * y));
-  } else if (p.bathy_flag == SWM_BATHY_BUMP) {
-    double r2 = x * x + y * y;
-    if (r2 < 1) {
-      double d = 1.0 - r2;
-      double e = exp(1.0 - 1.0 / d);
-      *bx = -(2.0 * x / (d * d) * e);
-      *by = -(2.0 * y / (d * d) * e);
-    }
-  } else if (p.bathy_flag == SWM_BATHY_GAUSS) {
-    const double A = p.bathy_par[0], ax = p.bathy_par[1], cx = p.bathy_par[2];
-    const double ay = p.bathy_par[3], cy = p.bathy_par[4];
-    double dxv = x - cx, dyv = y - cy;
-    double e = exp(-(ax * (dxv * dxv) + ay * (dyv * dyv)));
-    double B = A * e;
-    *bx = (-2.0 * ax * dxv) * B;
-    *by = (-2.0 * ay * dyv) * B;
-  }
-}
-
 // The split and FMA forms use the reciprocal Patankar weights and the 1/Diagonal
 // stencil Jacobi; the FP64 form keeps every division of the reference.
 static bool fast_patankar(const swm_params& p) {
@@ -210,8 +166,8 @@ static RhsArgs make_rhs_args(swm_solver* s, const double* h, const double* hu, c
     a.fy_wb = s->fywb;
     a.s_wb = s->swb;
   }
-  a.gauss_ex = s->gex;
-  a.gauss_ey = s->gey;
+  a.src_col = s->src_col;
+  a.src_row = s->src_row;
   a.bgrad = s->bgrad;
   return a;
 }
@@ -415,19 +371,8 @@ int swm_create(const swm_params* p, swm_handle* out) {
   s->ny = p->ny;
   s->N = (size_t)p->nx * p->ny;
   // mesh.f90:58-60 and quadrature
-  Grid& gr = s->gr;
-  gr.nx = s->nx;
-  gr.ny = s->ny;
-  gr.x0 = p->x0[0];
-  gr.y0 = p->x0[1];
-  gr.dx = fabs(fabs(p->x1[0] - p->x0[0])) / ((double)s->nx);
-  gr.dy = fabs(fabs(p->x1[1] - p->x0[1])) / ((double)s->ny);
-  gr.g = p->g;
-  gr.bathy = p->bathy_flag;
-  for (int k = 0; k < 5; ++k) gr.bp[k] = p->bathy_par[k];
-  quadrature(gr.qn, gr.qw);
-  for (int a = 0; a < 4; ++a)
-    for (int b = 0; b < 4; ++b) gr.wgp[a][b] = gr.qw[a] * gr.qw[b];
+  s->gr = host_grid(*p);
+  const Grid& gr = s->gr;
 
   auto cleanup = [&](int code) {
     swm_destroy(s);
@@ -523,46 +468,23 @@ int swm_create(const swm_params* p, swm_handle* out) {
         cudaMemcpy(s->cols, cl.data(), sizeof(int) * 5 * N, cudaMemcpyHostToDevice) != cudaSuccess)
       return cleanup(fail(SWM_ERR_CUDA, "CSR upload failed"));
   }
-  if (p->bathy_flag == SWM_BATHY_GAUSS && p->precision != SWM_PREC_FP64) {
-    // separable Gaussian factors at the Gauss nodes (split and FMA forms)
-    int rc2 = s->dalloc(&s->gex, 4 * nx);
-    if (!rc2) rc2 = s->dalloc(&s->gey, 4 * ny);
+  if (separable_source(*p)) {
+    std::vector<double> col, row;
+    host_source_factors(*p, gr, col, row);
+    int rc2 = s->dalloc(&s->src_col, col.size());
+    if (!rc2) rc2 = s->dalloc(&s->src_row, row.size());
     if (rc2) return cleanup(rc2);
-    std::vector<double> ex(4 * nx), ey(4 * ny);
-    for (size_t i = 0; i < nx; ++i)
-      for (int q = 0; q < 4; ++q) {
-        double d = host_gp(gr.x0, gr.dx, (int)i, gr.qn[q]) - gr.bp[2];
-        ex[4 * i + q] = exp(-(gr.bp[1] * (d * d)));
-      }
-    for (size_t j = 0; j < ny; ++j)
-      for (int q = 0; q < 4; ++q) {
-        double d = host_gp(gr.y0, gr.dy, (int)j, gr.qn[q]) - gr.bp[4];
-        ey[4 * j + q] = exp(-(gr.bp[3] * (d * d)));
-      }
-    cudaMemcpy(s->gex, ex.data(), sizeof(double) * 4 * nx, cudaMemcpyHostToDevice);
-    cudaMemcpy(s->gey, ey.data(), sizeof(double) * 4 * ny, cudaMemcpyHostToDevice);
-  }
-  const bool full_table =
-      p->bathy_flag > 0 && (p->precision == SWM_PREC_FP64 || p->bathy_flag != SWM_BATHY_GAUSS);
-  if (full_table) {  // b_x, b_y at the 16 interior Gauss points, host libm (equation.f90:451-509)
-    int rc2 = s->dalloc(&s->bgrad, 32 * N);
+    if (cudaMemcpy(s->src_col, col.data(), sizeof(double) * col.size(), cudaMemcpyHostToDevice) !=
+            cudaSuccess ||
+        cudaMemcpy(s->src_row, row.data(), sizeof(double) * row.size(), cudaMemcpyHostToDevice) !=
+            cudaSuccess)
+      return cleanup(fail(SWM_ERR_CUDA, "bathymetry factor upload failed"));
+  } else if (full_source_table(*p)) {  // host libm (equation.f90:451-509)
+    std::vector<double> tab;
+    host_bgrad_table(*p, gr, tab);
+    int rc2 = s->dalloc(&s->bgrad, tab.size());
     if (rc2) return cleanup(rc2);
-    std::vector<double> tab(32 * N);
-    std::vector<double> X(4 * nx), Y(4 * ny);
-    for (size_t i = 0; i < nx; ++i)
-      for (int q = 0; q < 4; ++q) X[4 * i + q] = host_gp(gr.x0, gr.dx, (int)i, gr.qn[q]);
-    for (size_t j = 0; j < ny; ++j)
-      for (int q = 0; q < 4; ++q) Y[4 * j + q] = host_gp(gr.y0, gr.dy, (int)j, gr.qn[q]);
-    for (int a = 0; a < 4; ++a)
-      for (int b = 0; b < 4; ++b)
-        for (size_t j = 0; j < ny; ++j)
-          for (size_t i = 0; i < nx; ++i) {
-            double bx, by;
-            host_bathy_grad(*p, X[4 * i + a], Y[4 * j + b], &bx, &by);
-            tab[((a * 4 + b) * 2 + 0) * N + j * nx + i] = bx;
-            tab[((a * 4 + b) * 2 + 1) * N + j * nx + i] = by;
-          }
-    if (cudaMemcpy(s->bgrad, tab.data(), sizeof(double) * 32 * N, cudaMemcpyHostToDevice) !=
+    if (cudaMemcpy(s->bgrad, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice) !=
         cudaSuccess)
       return cleanup(fail(SWM_ERR_CUDA, "bathymetry table upload failed"));
   }

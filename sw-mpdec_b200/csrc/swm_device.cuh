@@ -2,8 +2,9 @@
 //
 // The three precision forms share this code:
 //   EXACT  (FP64, translation unit built with -fmad=false): the reference's
-//          expression order and IEEE divisions, so that results match the CPU
-//          restatement of the Fortran bit for bit where no libm call is involved;
+//          expression order and correctly rounded divisions (div_rn), so that
+//          results match the CPU restatement of the Fortran bit for bit where no
+//          libm call is involved;
 //   FAST   (FP64, FMA contraction): WENO weights use one reciprocal per
 //          smoothness indicator and one per Gauss point instead of six
 //          divisions per point;
@@ -25,6 +26,9 @@ constexpr double kWenoEps = 1.0e-24;
 // a flat stencil's weights into inf/inf.  (1e-18)^2 = 1e-36 is a normal float.
 constexpr float kWenoEpsF = 1.0e-18f;
 constexpr double kWLobatto = 1. / 12.;
+// limiter denominator 1 - 2 wL and its correctly rounded reciprocal
+constexpr double kCsiDen = 1. - 2. * kWLobatto;
+constexpr double kCsiRcp = 1. / kCsiDen;
 
 // Bathymetry kinds (swm.h SWM_BATHY_*)
 enum { BATHY_FLAT = 0, BATHY_SINCOS = 1, BATHY_BUMP = 2, BATHY_GAUSS = 3 };
@@ -33,6 +37,7 @@ struct Grid {
   int nx, ny;
   double x0, y0;
   double dx, dy;
+  double rdx, rdy;  // 1/dx, 1/dy (the split and FMA forms multiply by these)
   double g;
   int bathy;
   double bp[5];  // Gaussian A, ax, cx, ay, cy
@@ -48,8 +53,42 @@ __device__ __forceinline__ int wrap(int i, int n) {
 __device__ __forceinline__ double dmax(double a, double b) { return (a > b) ? a : b; }
 __device__ __forceinline__ double dmin(double a, double b) { return (a < b) ? a : b; }
 
-__device__ __forceinline__ double rcp_(double x) { return 1.0 / x; }
-__device__ __forceinline__ float rcp_(float x) { return __fdividef(1.0f, x); }
+// Reciprocals of the non-EXACT WENO weights: the correctly rounded FP64 reciprocal,
+// and the hardware approximation in FP32 (relative error ~2^-23; its arguments are
+// normal: eps_f^2 = 1e-36 <= d and the weight sums are bounded by 1/d).
+__device__ __forceinline__ double rcp_(double x) { return __drcp_rn(x); }
+__device__ __forceinline__ float rcp_(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
+// Correctly rounded x / y from a shared correctly rounded reciprocal r = RN(1/y):
+// two residual corrections with FMA (Markstein, IBM J. Res. Dev. 34(1), 1990;
+// Theorem 8.10 of Muller et al., Handbook of Floating-Point Arithmetic): with r
+// correctly rounded and q faithful, q + RN(x - q y) r rounds to RN(x / y), provided
+// the residual x - q y is exact and the quotient normal.  mk_range() bounds the
+// operands so that this holds: x, y in [2^-400, 2^400) gives quotients in
+// (2^-800, 2^800) and residuals far above the subnormal range.
+__device__ __forceinline__ bool mk_range(double x) {
+  return ((unsigned)(__double2hiint(x) >> 20) & 0x7ffu) - 623u < 800u;
+}
+__device__ __forceinline__ double div_mk(double x, double y, double r) {
+  double q = x * r;
+  double e = fma(-q, y, x);
+  q = fma(e, r, q);
+  e = fma(-q, y, x);
+  return fma(e, r, q);
+}
+// The IEEE division, kept out of line: it only serves operands outside mk_range.
+static __device__ __noinline__ double div_ieee(double x, double y) { return x / y; }
+// x / y for any operands; a zero numerator gives x * r, the correctly signed zero
+// (NaN for y = 0 or NaN).
+__device__ __forceinline__ double div_rn(double x, double y, double r) {
+  if (__builtin_expect(mk_range(x) && mk_range(y), 1)) return div_mk(x, y, r);
+  if (x == 0.0) return x * r;
+  return div_ieee(x, y);
+}
 
 template <typename T>
 __device__ __forceinline__ T weno_eps();
@@ -89,14 +128,25 @@ __device__ __forceinline__ void weno_d(T qm2, T qm1, T q0, T qp1, T qp2, T& d1, 
   d3 = t3 * t3;
 }
 
-// Nonlinear combination of one reconstruction point.
+// How the WENO weights divide: products with reciprocals (non-EXACT forms), or the
+// reference's quotients, correctly rounded from shared reciprocals (EXACT, when the
+// smoothness indicators are in mk_range) or by IEEE division (EXACT otherwise).
+enum { kDivRcp = 0, kDivMk = 1, kDivIeee = 2 };
+
+// Nonlinear combination of one reconstruction point, i_k = RN(1/d_k).
 //  EXACT: omega_k = alpha_k/(alpha1+alpha2+alpha3), alpha_k = gamma_k/d_k
-//         (reconstruction.f90:716-728), literal order.
-//  else : the same weights from shared reciprocals i_k = 1/d_k.
-template <typename T, bool EXACT>
+//         (reconstruction.f90:716-728), literal order.  With d_k in
+//         [2^-400, 2^400), alpha_k and their sum lie in [2^-405, 2^402], so every
+//         quotient (>= 2^-807) and residual stays normal and div_mk is exact.
+//  else : the same weights as products with the reciprocals.
+template <typename T, int DIV>
 __device__ __forceinline__ T weno_point(T g1, T g2, T g3, T d1, T d2, T d3, T i1, T i2, T i3, T W1,
                                         T W2, T W3) {
-  if (EXACT) {
+  if constexpr (DIV == kDivMk) {
+    T a1 = div_mk(g1, d1, i1), a2 = div_mk(g2, d2, i2), a3 = div_mk(g3, d3, i3);
+    const T s = a1 + a2 + a3, rs = rcp_(s);
+    return div_mk(a1, s, rs) * W1 + div_mk(a2, s, rs) * W2 + div_mk(a3, s, rs) * W3;
+  } else if constexpr (DIV == kDivIeee) {
     T a1 = g1 / d1, a2 = g2 / d2, a3 = g3 / d3;
     return a1 / (a1 + a2 + a3) * W1 + a2 / (a1 + a2 + a3) * W2 + a3 / (a1 + a2 + a3) * W3;
   } else {
@@ -105,12 +155,24 @@ __device__ __forceinline__ T weno_point(T g1, T g2, T g3, T d1, T d2, T d3, T i1
   }
 }
 
-// WENO5_FirstSweep (reconstruction.f90:673-755): cell-face means at x_{i-1/2}, x_{i+1/2}.
-template <typename T, bool EXACT>
-__device__ __forceinline__ void weno5_first(T qm2, T qm1, T q0, T qp1, T qp2, T& wm, T& wp) {
-  T d1, d2, d3, i1 = T(0), i2 = T(0), i3 = T(0);
+template <int DIV>
+__device__ __forceinline__ bool div_ok(double d1, double d2, double d3) {
+  return DIV != kDivMk || (mk_range(d1) && mk_range(d2) && mk_range(d3));
+}
+template <int DIV>
+__device__ __forceinline__ bool div_ok(float, float, float) {
+  return true;
+}
+
+// WENO5_FirstSweep (reconstruction.f90:673-755): cell-face means at x_{i-1/2},
+// x_{i+1/2}.  Returns false (nothing written) when kDivMk's range check fails.
+template <typename T, bool EXACT, int DIV>
+__device__ __forceinline__ bool weno5_first_div(T qm2, T qm1, T q0, T qp1, T qp2, T& wm, T& wp) {
+  T d1, d2, d3;
   weno_d<T, EXACT>(qm2, qm1, q0, qp1, qp2, d1, d2, d3);
-  if (!EXACT) {
+  if (!div_ok<DIV>(d1, d2, d3)) return false;
+  T i1 = T(0), i2 = T(0), i3 = T(0);
+  if constexpr (DIV != kDivIeee) {
     i1 = rcp_(d1);
     i2 = rcp_(d2);
     i3 = rcp_(d3);
@@ -119,24 +181,27 @@ __device__ __forceinline__ void weno5_first(T qm2, T qm1, T q0, T qp1, T qp2, T&
   T W1 = s6 * (-qm2 + T(5.0) * qm1 + T(2.0) * q0);
   T W2 = s6 * (T(2.0) * qm1 + T(5.0) * q0 - qp1);
   T W3 = s6 * (T(11.0) * q0 - T(7.0) * qp1 + T(2.0) * qp2);
-  wm = weno_point<T, EXACT>(T(3.0) / T(10.0), T(3.0) / T(5.0), T(1.0) / T(10.0), d1, d2, d3, i1, i2,
-                            i3, W1, W2, W3);
+  wm = weno_point<T, DIV>(T(3.0) / T(10.0), T(3.0) / T(5.0), T(1.0) / T(10.0), d1, d2, d3, i1, i2,
+                          i3, W1, W2, W3);
   W1 = s6 * (T(2.0) * qm2 - T(7.0) * qm1 + T(11.0) * q0);
   W2 = s6 * (-qm1 + T(5.0) * q0 + T(2.0) * qp1);
   W3 = s6 * (T(2.0) * q0 + T(5.0) * qp1 - qp2);
-  wp = weno_point<T, EXACT>(T(1.0) / T(10.0), T(3.0) / T(5.0), T(3.0) / T(10.0), d1, d2, d3, i1, i2,
-                            i3, W1, W2, W3);
+  wp = weno_point<T, DIV>(T(1.0) / T(10.0), T(3.0) / T(5.0), T(3.0) / T(10.0), d1, d2, d3, i1, i2,
+                          i3, W1, W2, W3);
+  return true;
 }
 
 // WENO5_SecondSweep (reconstruction.f90:999-1136): values at the 4 Gauss nodes.
 // Linear weights and sub-stencil coefficients are the reference's tabulated
 // constants (generated offline by weno-weights/WENO_double.m); the reference's
 // 0.0*Q(k) terms are omitted (they only change the sign of an exact zero).
-template <typename T, bool EXACT>
-__device__ __forceinline__ void weno5_second(T qm2, T qm1, T q0, T qp1, T qp2, T w[4]) {
-  T d1, d2, d3, i1 = T(0), i2 = T(0), i3 = T(0);
+template <typename T, bool EXACT, int DIV>
+__device__ __forceinline__ bool weno5_second_div(T qm2, T qm1, T q0, T qp1, T qp2, T w[4]) {
+  T d1, d2, d3;
   weno_d<T, EXACT>(qm2, qm1, q0, qp1, qp2, d1, d2, d3);
-  if (!EXACT) {
+  if (!div_ok<DIV>(d1, d2, d3)) return false;
+  T i1 = T(0), i2 = T(0), i3 = T(0);
+  if constexpr (DIV != kDivIeee) {
     i1 = rcp_(d1);
     i2 = rcp_(d2);
     i3 = rcp_(d3);
@@ -145,30 +210,88 @@ __device__ __forceinline__ void weno5_second(T qm2, T qm1, T q0, T qp1, T qp2, T
   W1 = T(-0.1642562761719537) * qm2 + T(0.7590807081409336) * qm1 + T(0.4051755680310201) * q0;
   W2 = T(0.2663118796250726) * qm1 + T(0.8979443965468811) * q0 - T(0.1642562761719537) * qp1;
   W3 = T(1.6968800354220990) * q0 - T(0.9631919150471715) * qp1 + T(0.2663118796250726) * qp2;
-  w[0] = weno_point<T, EXACT>(T(0.2658420974778319), T(0.6112504900322486), T(0.1229074124899195),
-                              d1, d2, d3, i1, i2, i3, W1, W2, W3);
+  w[0] = weno_point<T, DIV>(T(0.2658420974778319), T(0.6112504900322486), T(0.1229074124899195),
+                            d1, d2, d3, i1, i2, i3, W1, W2, W3);
   W1 = T(-0.1122135388132497) * qm2 + T(0.3944175994189276) * qm1 + T(0.7177959393943222) * q0;
   W2 = T(0.0577769829791784) * qm1 + T(1.0544365558340714) * q0 - T(0.1122135388132497) * qp1;
   W3 = T(1.2277675047716066) * q0 - T(0.2855444877507849) * qp1 + T(0.0577769829791784) * qp2;
-  w[1] = weno_point<T, EXACT>(T(0.1281641584355059), T(0.5219691498503563), T(0.3498666917141379),
-                              d1, d2, d3, i1, i2, i3, W1, W2, W3);
+  w[1] = weno_point<T, DIV>(T(0.1281641584355059), T(0.5219691498503563), T(0.3498666917141379),
+                            d1, d2, d3, i1, i2, i3, W1, W2, W3);
   W1 = T(0.0577769829791784) * qm2 - T(0.2855444877507849) * qm1 + T(1.2277675047716066) * q0;
   W2 = T(-0.1122135388132497) * qm1 + T(1.0544365558340714) * q0 + T(0.0577769829791784) * qp1;
   W3 = T(0.7177959393943222) * q0 + T(0.3944175994189276) * qp1 - T(0.1122135388132497) * qp2;
-  w[2] = weno_point<T, EXACT>(T(0.3498666917141379), T(0.5219691498503563), T(0.1281641584355059),
-                              d1, d2, d3, i1, i2, i3, W1, W2, W3);
+  w[2] = weno_point<T, DIV>(T(0.3498666917141379), T(0.5219691498503563), T(0.1281641584355059),
+                            d1, d2, d3, i1, i2, i3, W1, W2, W3);
   W1 = T(0.2663118796250726) * qm2 - T(0.9631919150471715) * qm1 + T(1.6968800354220990) * q0;
   W2 = T(-0.1642562761719537) * qm1 + T(0.8979443965468811) * q0 + T(0.2663118796250726) * qp1;
   W3 = T(0.4051755680310201) * q0 + T(0.7590807081409336) * qp1 - T(0.1642562761719537) * qp2;
-  w[3] = weno_point<T, EXACT>(T(0.1229074124899195), T(0.6112504900322486), T(0.2658420974778319),
-                              d1, d2, d3, i1, i2, i3, W1, W2, W3);
+  w[3] = weno_point<T, DIV>(T(0.1229074124899195), T(0.6112504900322486), T(0.2658420974778319),
+                            d1, d2, d3, i1, i2, i3, W1, W2, W3);
+  return true;
 }
 
-// ConsToPrim (equation.f90:912-945)
+// Out-of-line IEEE versions for EXACT reconstructions whose indicators leave mk_range
+// (results by value, so that the callers' arrays stay in registers).
+struct Weno2 {
+  double m, p;
+};
+struct Weno4 {
+  double w[4];
+};
+static __device__ __noinline__ Weno2 weno5_first_ieee(double qm2, double qm1, double q0, double qp1,
+                                               double qp2) {
+  Weno2 r;
+  weno5_first_div<double, true, kDivIeee>(qm2, qm1, q0, qp1, qp2, r.m, r.p);
+  return r;
+}
+static __device__ __noinline__ Weno4 weno5_second_ieee(double qm2, double qm1, double q0, double qp1,
+                                                double qp2) {
+  Weno4 r;
+  weno5_second_div<double, true, kDivIeee>(qm2, qm1, q0, qp1, qp2, r.w);
+  return r;
+}
+
+template <typename T, bool EXACT>
+__device__ __forceinline__ void weno5_first(T qm2, T qm1, T q0, T qp1, T qp2, T& wm, T& wp) {
+  if constexpr (EXACT) {
+    if (!weno5_first_div<T, true, kDivMk>(qm2, qm1, q0, qp1, qp2, wm, wp)) {
+      const Weno2 r = weno5_first_ieee(qm2, qm1, q0, qp1, qp2);
+      wm = r.m;
+      wp = r.p;
+    }
+  } else {
+    weno5_first_div<T, false, kDivRcp>(qm2, qm1, q0, qp1, qp2, wm, wp);
+  }
+}
+
+template <typename T, bool EXACT>
+__device__ __forceinline__ void weno5_second(T qm2, T qm1, T q0, T qp1, T qp2, T w[4]) {
+  if constexpr (EXACT) {
+    if (!weno5_second_div<T, true, kDivMk>(qm2, qm1, q0, qp1, qp2, w)) {
+      const Weno4 r = weno5_second_ieee(qm2, qm1, q0, qp1, qp2);
+#pragma unroll
+      for (int g = 0; g < 4; ++g) w[g] = r.w[g];
+    }
+  } else {
+    weno5_second_div<T, false, kDivRcp>(qm2, qm1, q0, qp1, qp2, w);
+  }
+}
+
+// ConsToPrim (equation.f90:912-945): u = hu / (h + MIN_DEPTH / h).  EXACT rounds
+// every quotient correctly (div_rn, one reciprocal of the desingularised depth for
+// both velocities); the other forms multiply by the reciprocals.  h = 0 gives
+// ht = inf and u = v = 0 in both.
+template <bool EXACT>
 __device__ __forceinline__ void cons_to_prim(double h, double hu, double hv, double& u, double& v) {
-  double ht = h + kMinDepth / h;
-  u = hu / ht;
-  v = hv / ht;
+  if constexpr (EXACT) {
+    const double ht = h + div_rn(kMinDepth, h, __drcp_rn(h)), rt = __drcp_rn(ht);
+    u = div_rn(hu, ht, rt);
+    v = div_rn(hv, ht, rt);
+  } else {
+    const double rt = __drcp_rn(h + kMinDepth * __drcp_rn(h));
+    u = hu * rt;
+    v = hv * rt;
+  }
 }
 
 // Rusanov flux in the face-normal frame: EvaluateFlux1D + WaveSpeeds1D +
@@ -209,7 +332,7 @@ __device__ __forceinline__ void limit_h(const Grid& gr, double Vc, double wm[4],
     alpha = alpha + gr.qw[g] * wm[g];
     beta = beta + gr.qw[g] * wp[g];
   }
-  double csi = (Vc - kWLobatto * alpha - kWLobatto * beta) / (1. - 2. * kWLobatto);
+  double csi = div_rn(Vc - kWLobatto * alpha - kWLobatto * beta, kCsiDen, kCsiRcp);
 #pragma unroll
   for (int g = 0; g < 4; ++g) {
     double mmin = csi;
@@ -237,7 +360,7 @@ __device__ __forceinline__ void limit_h_dev(const Grid& gr, double Vc, const flo
     alpha = alpha + gr.qw[g] * (double)dm[g];
     beta = beta + gr.qw[g] * (double)dp[g];
   }
-  double csi = -(kWLobatto * alpha + kWLobatto * beta) / (1. - 2. * kWLobatto);
+  double csi = -(kWLobatto * alpha + kWLobatto * beta) * kCsiRcp;
 #pragma unroll
   for (int g = 0; g < 4; ++g) {
     double mmin = csi;
@@ -251,42 +374,6 @@ __device__ __forceinline__ void limit_h_dev(const Grid& gr, double Vc, const flo
     wp[g] = Vc + theta * (double)dp[g];
     wm[g] = Vc + theta * (double)dm[g];
   }
-}
-
-// Bathymetry gradient (equation.f90:451-509; flag 3 is the Gaussian used by the
-// benchmark cases).
-__device__ __forceinline__ void bathy_grad(const Grid& gr, double x, double y, double& bx,
-                                           double& by) {
-  const double PI = 3.141592653589793;  // ACOS(-1.0) in FP64
-  bx = 0.;
-  by = 0.;
-  if (gr.bathy == BATHY_SINCOS) {
-    bx = 0.1 * 2. * PI * cos(2. * PI * x) * cos(2. * PI * y);
-    by = -(0.1 * 2. * PI * sin(2. * PI * x) * sin(2. * PI * y));
-  } else if (gr.bathy == BATHY_BUMP) {
-    double r2 = x * x + y * y;
-    if (r2 < 1) {
-      double d = 1.0 - r2;
-      double e = exp(1.0 - 1.0 / d);
-      bx = -(2.0 * x / (d * d) * e);
-      by = -(2.0 * y / (d * d) * e);
-    }
-  } else if (gr.bathy == BATHY_GAUSS) {
-    double dxv = x - gr.bp[2], dyv = y - gr.bp[4];
-    double e = exp(-(gr.bp[1] * (dxv * dxv) + gr.bp[3] * (dyv * dyv)));
-    double B = gr.bp[0] * e;
-    bx = (-2.0 * gr.bp[1] * dxv) * B;
-    by = (-2.0 * gr.bp[3] * dyv) * B;
-  }
-}
-
-// x (d=0) or y (d=1) coordinate of Gauss node q of cell index c (0-based),
-// mesh.f90:64,70,142: node = x0 + REAL(ii)*dx; bary = node + 0.5 dx; gp = bary + qn dx.
-__device__ __forceinline__ double gp_coord(const Grid& gr, int d, int c, int q) {
-  double x0 = d ? gr.y0 : gr.x0, h = d ? gr.dy : gr.dx;
-  double node = x0 + ((double)c) * h;
-  double bary = node + 0.5 * h;
-  return bary + gr.qn[q] * h;
 }
 
 }  // namespace swm

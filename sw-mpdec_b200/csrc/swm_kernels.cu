@@ -72,7 +72,7 @@ __global__ void dt_kernel(const DtArgs a) {
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
     double h = a.h[k], hu = a.hu[k], hv = a.hv[k], u, v;
     if (!(h >= 0.0) || !isfinite(h) || !isfinite(hu) || !isfinite(hv)) bad = 1;
-    cons_to_prim(h, hu, hv, u, v);
+    cons_to_prim<true>(h, hu, hv, u, v);
     double c = sqrt(a.g * h);
     lx = dmax(lx, fabs(u + c));
     ly = dmax(ly, fabs(v + c));
@@ -130,7 +130,7 @@ __global__ void planes_to_ghosted_kernel(const double* h, const double* hu, cons
     G[3 * (size_t)k + 2] = c;
     if (Vg) {
       double u, v;
-      cons_to_prim(a, b, c, u, v);
+      cons_to_prim<true>(a, b, c, u, v);
       Vg[3 * (size_t)k] = a;
       Vg[3 * (size_t)k + 1] = u;
       Vg[3 * (size_t)k + 2] = v;
@@ -987,7 +987,7 @@ __global__ void __launch_bounds__(128)
   if (c < q.nx * q.ny) {
     double h = q.h[c], hu = q.hu[c], hv = q.hv[c], u, v;
     if (!(h >= 0.0) || !isfinite(h) || !isfinite(hu) || !isfinite(hv)) b = 1;
-    cons_to_prim(h, hu, hv, u, v);
+    cons_to_prim<true>(h, hu, hv, u, v);
     double cc = sqrt(q.g * h);
     lx = fabs(u + cc);
     ly = fabs(v + cc);

@@ -39,8 +39,11 @@ struct RhsArgs {
   const double* fx_wb;  // nullable: WB reference fluxes, same layouts
   const double* fy_wb;
   const double* s_wb;
-  const double* gauss_ex;  // nullable: Gaussian factors exp(-ax (x_q-cx)^2) [nx][4]
-  const double* gauss_ey;  // nullable: exp(-ay (y_q-cy)^2) [ny][4]
+  // nullable: separable source factors with the Gauss weights folded in,
+  // src_col [nx][2][4] = {w_a P(x_a), w_a R(x_a)}, src_row [ny][2][4] =
+  // {w_b Q(y_b), w_b T(y_b)} for b_x = P Q, b_y = R T (split and FMA forms)
+  const double* src_col;
+  const double* src_row;
   // nullable: b_x, b_y at the 16 interior Gauss points of every cell, evaluated on the
   // host with the analytic formula (equation.f90:451-509), planes [4][4][2][ny*nx]
   const double* bgrad;
@@ -96,12 +99,22 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const i
   const int tid = threadIdx.x;
 
   // ---- load the haloed tile, V = ConsToPrim(U) (equation.f90:778-782) ----
+  // Periodic wrap: one conditional add/subtract when the grid is at least one haloed
+  // tile wide, the general modulo otherwise.
+  const bool wide = nx >= VX && ny >= VY;
   for (int it = tid; it < VY * VX; it += NT) {
     int cx = it % VX, cy = it / VX;
-    int gi = wrap(i0 - 3 + cx, nx), gj = wrap(j0 - 3 + cy, ny);
+    int gi = i0 - 3 + cx, gj = j0 - 3 + cy;
+    if (wide) {
+      gi += gi < 0 ? nx : (gi >= nx ? -nx : 0);
+      gj += gj < 0 ? ny : (gj >= ny ? -ny : 0);
+    } else {
+      gi = wrap(gi, nx);
+      gj = wrap(gj, ny);
+    }
     size_t k = (size_t)gj * nx + gi;
     double h = a.h[k], hu = a.hu[k], hv = a.hv[k], u, v;
-    cons_to_prim(h, hu, hv, u, v);
+    cons_to_prim<EX>(h, hu, hv, u, v);
     sV[(0 * VY + cy) * VX + cx] = h;
     sV[(1 * VY + cy) * VX + cx] = u;
     sV[(2 * VY + cy) * VX + cx] = v;
@@ -339,28 +352,42 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const i
           for (int aa = 0; aa < 4; ++aa) hq[aa][b] = (double)w[aa];
         }
       }
-      // S = sum_{a (x-GP)} sum_{b (y-GP)} W(a,b) * SourceFunc (equation.f90:380-388, :408-410)
+      if (!EX && a.src_col) {
+        // separable gradient: S_hu = -g sum_a Pw_a sum_b Qw_b h_ab,
+        //                     S_hv = -g sum_b Tw_b sum_a Rw_a h_ab
+        const double* pc = a.src_col + 8 * (size_t)gi;
+        const double* pr = a.src_row + 8 * (size_t)gj;
+        double s1 = 0.0, s2 = 0.0;
 #pragma unroll
-      for (int aa = 0; aa < 4; ++aa) {
-        double X = gp_coord(gr, 0, gi, aa);
+        for (int aa = 0; aa < 4; ++aa) {
+          double in = 0.0;
+#pragma unroll
+          for (int b = 0; b < 4; ++b) in = fma(__ldg(pr + b), hq[aa][b], in);
+          s1 = fma(__ldg(pc + aa), in, s1);
+        }
 #pragma unroll
         for (int b = 0; b < 4; ++b) {
-          double bx, by;
-          if (a.bgrad) {  // host-tabulated analytic gradient, [x-GP][y-GP][comp][cell]
-            const size_t nc = (size_t)nx * ny, cell = (size_t)gj * nx + gi;
-            bx = a.bgrad[((aa * 4 + b) * 2 + 0) * nc + cell];
-            by = a.bgrad[((aa * 4 + b) * 2 + 1) * nc + cell];
-          } else if (gr.bathy == BATHY_GAUSS && a.gauss_ex) {
-            double Y = gp_coord(gr, 1, gj, b);
-            double B = gr.bp[0] * (a.gauss_ex[gi * 4 + aa] * a.gauss_ey[gj * 4 + b]);
-            bx = (-2.0 * gr.bp[1] * (X - gr.bp[2])) * B;
-            by = (-2.0 * gr.bp[3] * (Y - gr.bp[4])) * B;
-          } else {
-            bathy_grad(gr, X, gp_coord(gr, 1, gj, b), bx, by);
+          double in = 0.0;
+#pragma unroll
+          for (int aa = 0; aa < 4; ++aa) in = fma(__ldg(pc + 4 + aa), hq[aa][b], in);
+          s2 = fma(__ldg(pr + 4 + b), in, s2);
+        }
+        S1 = -gr.g * s1;
+        S2 = -gr.g * s2;
+      } else {
+        // S = sum_{a (x-GP)} sum_{b (y-GP)} W(a,b) * SourceFunc (equation.f90:380-388,
+        // :408-410), gradient from the host table [x-GP][y-GP][comp][cell]
+        const size_t nc = (size_t)nx * ny, cell = (size_t)gj * nx + gi;
+#pragma unroll
+        for (int aa = 0; aa < 4; ++aa) {
+#pragma unroll
+          for (int b = 0; b < 4; ++b) {
+            const double bx = a.bgrad[((aa * 4 + b) * 2 + 0) * nc + cell];
+            const double by = a.bgrad[((aa * 4 + b) * 2 + 1) * nc + cell];
+            double gh = gr.g * hq[aa][b];
+            S1 = S1 + gr.wgp[aa][b] * (-(gh * bx));
+            S2 = S2 + gr.wgp[aa][b] * (-(gh * by));
           }
-          double gh = gr.g * hq[aa][b];
-          S1 = S1 + gr.wgp[aa][b] * (-(gh * bx));
-          S2 = S2 + gr.wgp[aa][b] * (-(gh * by));
         }
       }
     }
@@ -384,9 +411,17 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const i
         s[v] = s[v] - a.s_wb[v * sc + kc];
       }
     }
-    // Ut(2:3) = S - (FX(i)-FX(i-1))/dx - (FY(j)-FY(j-1))/dy (finitevolume.f90:525-527)
-    a.ut_hu[kc] = s[1] - (fxr[1] - fxl[1]) / gr.dx - (fyt[1] - fyb[1]) / gr.dy;
-    a.ut_hv[kc] = s[2] - (fxr[2] - fxl[2]) / gr.dx - (fyt[2] - fyb[2]) / gr.dy;
+    // Ut(2:3) = S - (FX(i)-FX(i-1))/dx - (FY(j)-FY(j-1))/dy (finitevolume.f90:525-527);
+    // EXACT rounds the quotients correctly from rdx = RN(1/dx), the others multiply.
+    if constexpr (EX) {
+      a.ut_hu[kc] = s[1] - div_rn(fxr[1] - fxl[1], gr.dx, gr.rdx) -
+                    div_rn(fyt[1] - fyb[1], gr.dy, gr.rdy);
+      a.ut_hv[kc] = s[2] - div_rn(fxr[2] - fxl[2], gr.dx, gr.rdx) -
+                    div_rn(fyt[2] - fyb[2], gr.dy, gr.rdy);
+    } else {
+      a.ut_hu[kc] = s[1] - (fxr[1] - fxl[1]) * gr.rdx - (fyt[1] - fyb[1]) * gr.rdy;
+      a.ut_hv[kc] = s[2] - (fxr[2] - fxl[2]) * gr.rdx - (fyt[2] - fyb[2]) * gr.rdy;
+    }
     a.fxm[kx] = fxl[0];
     a.fym[ky] = fyb[0];
     if (gi == nx - 1) a.fxm[kx + 1] = fxr[0];
