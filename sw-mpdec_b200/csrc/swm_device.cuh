@@ -277,6 +277,119 @@ __device__ __forceinline__ void weno5_second(T qm2, T qm1, T q0, T qp1, T qp2, T
   }
 }
 
+// ---------------------------------------------------------------------------------
+// Packed FP32 pairs for the split form: sm_100's f32x2 add/sub/mul/fma instructions
+// carry two independent reconstructions per issued instruction (the two faces of a
+// cell, or two neighbouring stencils).  The formulas are the non-EXACT ones above
+// with the 1/6 of the first sweep folded into its coefficients.
+struct f2 {
+  unsigned long long v;
+};
+__device__ __forceinline__ f2 f2_pack(float lo, float hi) {
+  f2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r.v) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ void f2_unpack(f2 a, float& lo, float& hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(a.v));
+}
+__device__ __forceinline__ f2 f2_splat(float c) { return f2_pack(c, c); }
+__device__ __forceinline__ f2 fma2(f2 a, f2 b, f2 c) {
+  f2 d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d.v) : "l"(a.v), "l"(b.v), "l"(c.v));
+  return d;
+}
+__device__ __forceinline__ f2 mul2(f2 a, f2 b) {
+  f2 d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d.v) : "l"(a.v), "l"(b.v));
+  return d;
+}
+__device__ __forceinline__ f2 add2(f2 a, f2 b) {
+  f2 d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d.v) : "l"(a.v), "l"(b.v));
+  return d;
+}
+__device__ __forceinline__ f2 sub2(f2 a, f2 b) {
+  f2 d;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d.v) : "l"(a.v), "l"(b.v));
+  return d;
+}
+__device__ __forceinline__ f2 rcp2(f2 a) {
+  float lo, hi;
+  f2_unpack(a, lo, hi);
+  return f2_pack(rcp_(lo), rcp_(hi));
+}
+// c1 x1 + c2 x2 + c3 x3 with scalar coefficients
+__device__ __forceinline__ f2 lin3(float c1, f2 x1, float c2, f2 x2, float c3, f2 x3) {
+  return fma2(f2_splat(c3), x3, fma2(f2_splat(c2), x2, mul2(f2_splat(c1), x1)));
+}
+
+// reciprocals of the squared smoothness indicators (sum-of-squares form)
+__device__ __forceinline__ void weno_rd_x2(f2 qm2, f2 qm1, f2 q0, f2 qp1, f2 qp2, f2& i1, f2& i2,
+                                           f2& i3) {
+  const f2 m2 = f2_splat(-2.f), m4 = f2_splat(-4.f), c3 = f2_splat(3.f);
+  const f2 c13 = f2_splat(13.f / 12.f), c4 = f2_splat(0.25f), eps = f2_splat(kWenoEpsF);
+  const f2 s1 = add2(fma2(m2, qm1, qm2), q0), r1 = fma2(c3, q0, fma2(m4, qm1, qm2));
+  const f2 s2 = add2(fma2(m2, q0, qm1), qp1), r2 = sub2(qm1, qp1);
+  const f2 s3 = add2(fma2(m2, qp1, q0), qp2), r3 = fma2(c3, q0, fma2(m4, qp1, qp2));
+  const f2 t1 = add2(eps, fma2(mul2(c13, s1), s1, mul2(mul2(c4, r1), r1)));
+  const f2 t2 = add2(eps, fma2(mul2(c13, s2), s2, mul2(mul2(c4, r2), r2)));
+  const f2 t3 = add2(eps, fma2(mul2(c13, s3), s3, mul2(mul2(c4, r3), r3)));
+  i1 = rcp2(mul2(t1, t1));
+  i2 = rcp2(mul2(t2, t2));
+  i3 = rcp2(mul2(t3, t3));
+}
+
+__device__ __forceinline__ f2 weno_point_x2(float g1, float g2, float g3, f2 i1, f2 i2, f2 i3, f2 W1,
+                                            f2 W2, f2 W3) {
+  const f2 a1 = mul2(f2_splat(g1), i1), a2 = mul2(f2_splat(g2), i2), a3 = mul2(f2_splat(g3), i3);
+  const f2 num = fma2(a3, W3, fma2(a2, W2, mul2(a1, W1)));
+  return mul2(num, rcp2(add2(add2(a1, a2), a3)));
+}
+
+// Two first sweeps (reconstruction.f90:673-755).
+__device__ __forceinline__ void weno5_first_x2(f2 qm2, f2 qm1, f2 q0, f2 qp1, f2 qp2, f2& wm,
+                                               f2& wp) {
+  f2 i1, i2, i3;
+  weno_rd_x2(qm2, qm1, q0, qp1, qp2, i1, i2, i3);
+  const float s6 = 1.f / 6.f;
+  f2 W1 = lin3(-s6, qm2, 5.f * s6, qm1, 2.f * s6, q0);
+  f2 W2 = lin3(2.f * s6, qm1, 5.f * s6, q0, -s6, qp1);
+  f2 W3 = lin3(11.f * s6, q0, -7.f * s6, qp1, 2.f * s6, qp2);
+  wm = weno_point_x2(0.3f, 0.6f, 0.1f, i1, i2, i3, W1, W2, W3);
+  W1 = lin3(2.f * s6, qm2, -7.f * s6, qm1, 11.f * s6, q0);
+  W2 = lin3(-s6, qm1, 5.f * s6, q0, 2.f * s6, qp1);
+  W3 = lin3(2.f * s6, q0, 5.f * s6, qp1, -s6, qp2);
+  wp = weno_point_x2(0.1f, 0.6f, 0.3f, i1, i2, i3, W1, W2, W3);
+}
+
+// Two second sweeps (reconstruction.f90:999-1136), the coefficients of weno5_second.
+__device__ __forceinline__ void weno5_second_x2(f2 qm2, f2 qm1, f2 q0, f2 qp1, f2 qp2, f2 w[4]) {
+  f2 i1, i2, i3;
+  weno_rd_x2(qm2, qm1, q0, qp1, qp2, i1, i2, i3);
+  f2 W1, W2, W3;
+  W1 = lin3(-0.1642562761719537f, qm2, 0.7590807081409336f, qm1, 0.4051755680310201f, q0);
+  W2 = lin3(0.2663118796250726f, qm1, 0.8979443965468811f, q0, -0.1642562761719537f, qp1);
+  W3 = lin3(1.6968800354220990f, q0, -0.9631919150471715f, qp1, 0.2663118796250726f, qp2);
+  w[0] = weno_point_x2(0.2658420974778319f, 0.6112504900322486f, 0.1229074124899195f, i1, i2, i3,
+                       W1, W2, W3);
+  W1 = lin3(-0.1122135388132497f, qm2, 0.3944175994189276f, qm1, 0.7177959393943222f, q0);
+  W2 = lin3(0.0577769829791784f, qm1, 1.0544365558340714f, q0, -0.1122135388132497f, qp1);
+  W3 = lin3(1.2277675047716066f, q0, -0.2855444877507849f, qp1, 0.0577769829791784f, qp2);
+  w[1] = weno_point_x2(0.1281641584355059f, 0.5219691498503563f, 0.3498666917141379f, i1, i2, i3,
+                       W1, W2, W3);
+  W1 = lin3(0.0577769829791784f, qm2, -0.2855444877507849f, qm1, 1.2277675047716066f, q0);
+  W2 = lin3(-0.1122135388132497f, qm1, 1.0544365558340714f, q0, 0.0577769829791784f, qp1);
+  W3 = lin3(0.7177959393943222f, q0, 0.3944175994189276f, qp1, -0.1122135388132497f, qp2);
+  w[2] = weno_point_x2(0.3498666917141379f, 0.5219691498503563f, 0.1281641584355059f, i1, i2, i3,
+                       W1, W2, W3);
+  W1 = lin3(0.2663118796250726f, qm2, -0.9631919150471715f, qm1, 1.6968800354220990f, q0);
+  W2 = lin3(-0.1642562761719537f, qm1, 0.8979443965468811f, q0, 0.2663118796250726f, qp1);
+  W3 = lin3(0.4051755680310201f, q0, 0.7590807081409336f, qp1, -0.1642562761719537f, qp2);
+  w[3] = weno_point_x2(0.1229074124899195f, 0.6112504900322486f, 0.2658420974778319f, i1, i2, i3,
+                       W1, W2, W3);
+}
+
 // ConsToPrim (equation.f90:912-945): u = hu / (h + MIN_DEPTH / h).  EXACT rounds
 // every quotient correctly (div_rn, one reciprocal of the desingularised depth for
 // both velocities); the other forms multiply by the reciprocals.  h = 0 gives

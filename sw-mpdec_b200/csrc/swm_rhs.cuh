@@ -79,6 +79,56 @@ struct RhsSmem {
 namespace swm {
 namespace SWM_RHS_NS {
 
+// Gauss sum over the four lanes 4k..4k+3 of a face, in the reference's order
+// ((0 + t0) + t1) + t2) + t3 (finitevolume.f90:546-590); valid in lane 4k.  Every
+// lane of the warp must call it.
+__device__ __forceinline__ double quad_sum(double t) {
+  const double t1 = __shfl_down_sync(0xffffffffu, t, 1);
+  const double t2 = __shfl_down_sync(0xffffffffu, t, 2);
+  const double t3 = __shfl_down_sync(0xffffffffu, t, 3);
+  double s = __dadd_rn(0.0, t);
+  s = __dadd_rn(s, t1);
+  s = __dadd_rn(s, t2);
+  return __dadd_rn(s, t3);
+}
+
+// Gauss-summed fluxes of NF faces: whole faces (4 Gauss points in one thread,
+// conflict-free consecutive shared loads) while a full round of NT threads remains,
+// then the rest as (face, Gauss point) items, four lanes per face.  flux(f, g, F...)
+// evaluates one Gauss point, store(f, s0, s1, s2) keeps the sums.  Both paths round
+// every product and sum (no contraction), so a face shared by two tiles gets the same
+// flux from either, whichever path each tile takes for it.
+template <int NF, int NT, typename Flux, typename Store>
+__device__ __forceinline__ void face_pass(const Grid& gr, Flux&& flux, Store&& store) {
+  const int tid = threadIdx.x;
+  constexpr int FULL = (NF / NT) * NT, REST = NF - FULL;
+  for (int f = tid; f < FULL; f += NT) {
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+#pragma unroll
+    for (int g = 0; g < 4; ++g) {
+      double F0, F1, F2;
+      flux(f, g, F0, F1, F2);
+      s0 = __dadd_rn(s0, __dmul_rn(gr.qw[g], F0));
+      s1 = __dadd_rn(s1, __dmul_rn(gr.qw[g], F1));
+      s2 = __dadd_rn(s2, __dmul_rn(gr.qw[g], F2));
+    }
+    store(f, s0, s1, s2);
+  }
+  if constexpr (REST > 0) {
+    static_assert((4 * REST) % 32 == 0, "whole warps in the remainder");
+    for (int it0 = 0; it0 < 4 * REST; it0 += NT) {
+      if (it0 + (tid & ~31) >= 4 * REST) break;  // warp-uniform
+      const int it = it0 + tid, g = it & 3, f = FULL + (it >> 2);
+      double F0, F1, F2;
+      flux(f, g, F0, F1, F2);
+      const double w = gr.qw[g];
+      const double s0 = quad_sum(__dmul_rn(w, F0)), s1 = quad_sum(__dmul_rn(w, F1)),
+                   s2 = quad_sum(__dmul_rn(w, F2));
+      if (g == 0) store(f, s0, s1, s2);
+    }
+  }
+}
+
 // MODE: 0 FP64 (EXACT per translation unit), 1 SPLIT.  One CTA, tile origin (i0, j0).
 template <int MODE>
 __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const int j0) {
@@ -127,19 +177,33 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const i
     constexpr int FW = TX + 2, FH = TY + 4;  // first sweeps: cols i0-1..i0+TX, rows j0-2..j0+TY+1
     T* sTM = sF1;
     T* sTP = sF1 + 3 * FH * FW;
-    for (int it = tid; it < 3 * FH * FW; it += NT) {
-      int cc = it % FW, rest = it / FW, rr = rest % FH, v = rest / FH;
-      const double* q = &SV(v, rr + 1, cc);  // V cols (i0-1+cc)-2 .. +2 -> tile cols cc..cc+4
-      T wm, wp;
-      if constexpr (MODE == 1) {
-        double c0 = q[2];
-        weno5_first<T, false>((T)(q[0] - c0), (T)(q[1] - c0), T(0), (T)(q[3] - c0),
-                              (T)(q[4] - c0), wm, wp);
-      } else {
-        weno5_first<T, EX>((T)q[0], (T)q[1], (T)q[2], (T)q[3], (T)q[4], wm, wp);
+    if constexpr (MODE == 1) {
+      // two rows per item (packed pairs), deviations from each stencil's centre
+      static_assert(FH % 2 == 0, "row pairs");
+      constexpr int FH2 = FH / 2;
+      for (int it = tid; it < 3 * FH2 * FW; it += NT) {
+        int cc = it % FW, rest = it / FW, rp = rest % FH2, v = rest / FH2;
+        const int rr = 2 * rp;
+        const double* qa = &SV(v, rr + 1, cc);
+        const double* qb = &SV(v, rr + 2, cc);
+        const double ca = qa[2], cb = qb[2];
+        f2 q[5];
+#pragma unroll
+        for (int k = 0; k < 5; ++k) q[k] = f2_pack((float)(qa[k] - ca), (float)(qb[k] - cb));
+        f2 wm, wp;
+        weno5_first_x2(q[0], q[1], q[2], q[3], q[4], wm, wp);
+        f2_unpack(wm, sTM[(v * FH + rr) * FW + cc], sTM[(v * FH + rr + 1) * FW + cc]);
+        f2_unpack(wp, sTP[(v * FH + rr) * FW + cc], sTP[(v * FH + rr + 1) * FW + cc]);
       }
-      sTM[(v * FH + rr) * FW + cc] = wm;
-      sTP[(v * FH + rr) * FW + cc] = wp;
+    } else {
+      for (int it = tid; it < 3 * FH * FW; it += NT) {
+        int cc = it % FW, rest = it / FW, rr = rest % FH, v = rest / FH;
+        const double* q = &SV(v, rr + 1, cc);  // V cols (i0-1+cc)-2 .. +2 -> tile cols cc..cc+4
+        T wm, wp;
+        weno5_first<T, EX>((T)q[0], (T)q[1], (T)q[2], (T)q[3], (T)q[4], wm, wp);
+        sTM[(v * FH + rr) * FW + cc] = wm;
+        sTP[(v * FH + rr) * FW + cc] = wp;
+      }
     }
     __syncthreads();
     // second sweeps along y; cells: cols i0-1..i0+TX (cc), rows j0..j0+TY-1 (rr)
@@ -150,15 +214,16 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const i
       const double Vc = SV(v, rr + 3, cc + 2);
       if constexpr (MODE == 1) {
         float dm[4], dp[4];
-        T qm[5], qp[5];
+        f2 q[5], w[4];
 #pragma unroll
         for (int k = 0; k < 5; ++k) {
           T base = (T)(SV(v, rr + 1 + k, cc + 2) - Vc);  // row offset to the centre row
-          qm[k] = base + sTM[(v * FH + rr + k) * FW + cc];
-          qp[k] = base + sTP[(v * FH + rr + k) * FW + cc];
+          q[k] = f2_pack(base + sTM[(v * FH + rr + k) * FW + cc],
+                         base + sTP[(v * FH + rr + k) * FW + cc]);
         }
-        weno5_second<T, false>(qm[0], qm[1], qm[2], qm[3], qm[4], dm);
-        weno5_second<T, false>(qp[0], qp[1], qp[2], qp[3], qp[4], dp);
+        weno5_second_x2(q[0], q[1], q[2], q[3], q[4], w);
+#pragma unroll
+        for (int g = 0; g < 4; ++g) f2_unpack(w[g], dm[g], dp[g]);
         const int gc = i0 - 1 + cc;
         if (v == 0 && gc != nx) {
           limit_h_dev(gr, Vc, dm, dp, wmv, wpv);
@@ -191,25 +256,20 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const i
     }
     __syncthreads();
     // Rusanov at faces f = i0 .. i0+TX (ff), rows rr; left = WP(cell f-1) (cc = ff), right = WM(f)
-    for (int it = tid; it < TY * (TX + 1); it += NT) {
-      int ff = it % (TX + 1), rr = it / (TX + 1);
-      double s0 = 0.0, s1 = 0.0, s2 = 0.0;
-#pragma unroll
-      for (int g = 0; g < 4; ++g) {
-        const int L = rr * FW + ff, R = rr * FW + ff + 1;
-        double F0, F1, F2;
-        rusanov<MODE == 1>(gr.g, sW[((1 * 3 + 0) * 4 + g) * WC + L], sW[((1 * 3 + 1) * 4 + g) * WC + L],
-                sW[((1 * 3 + 2) * 4 + g) * WC + L], sW[((0 * 3 + 0) * 4 + g) * WC + R],
-                sW[((0 * 3 + 1) * 4 + g) * WC + R], sW[((0 * 3 + 2) * 4 + g) * WC + R], F0, F1,
-                F2);
-        s0 = s0 + gr.qw[g] * F0;
-        s1 = s1 + gr.qw[g] * F1;
-        s2 = s2 + gr.qw[g] * F2;
-      }
+    auto xface = [&](int f, int g, double& F0, double& F1, double& F2) {
+      const int ff = f % (TX + 1), rr = f / (TX + 1);
+      const int L = rr * FW + ff, R = rr * FW + ff + 1;
+      rusanov<MODE == 1>(gr.g, sW[((1 * 3 + 0) * 4 + g) * WC + L], sW[((1 * 3 + 1) * 4 + g) * WC + L],
+              sW[((1 * 3 + 2) * 4 + g) * WC + L], sW[((0 * 3 + 0) * 4 + g) * WC + R],
+              sW[((0 * 3 + 1) * 4 + g) * WC + R], sW[((0 * 3 + 2) * 4 + g) * WC + R], F0, F1, F2);
+    };
+    auto xstore = [&](int f, double s0, double s1, double s2) {
+      const int ff = f % (TX + 1), rr = f / (TX + 1);
       sFX[(0 * TY + rr) * (TX + 1) + ff] = s0;
       sFX[(1 * TY + rr) * (TX + 1) + ff] = s1;
       sFX[(2 * TY + rr) * (TX + 1) + ff] = s2;
-    }
+    };
+    face_pass<TY * (TX + 1), NT>(gr, xface, xstore);
     __syncthreads();
   }
 
@@ -218,20 +278,35 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const i
     constexpr int FW = TX + 4, FH = TY + 2;  // first sweeps: cols i0-2..i0+TX+1, rows j0-1..j0+TY
     T* sTM = sF1;
     T* sTP = sF1 + 3 * FH * FW;
-    for (int it = tid; it < 3 * FH * FW; it += NT) {
-      int cc = it % FW, rest = it / FW, rr = rest % FH, v = rest / FH;
-      // V rows (j0-1+rr)-2 .. +2 -> tile rows rr..rr+4; col (i0-2+cc) -> tile col cc+1
-      double q0 = SV(v, rr, cc + 1), q1 = SV(v, rr + 1, cc + 1), q2 = SV(v, rr + 2, cc + 1),
-             q3 = SV(v, rr + 3, cc + 1), q4 = SV(v, rr + 4, cc + 1);
-      T wm, wp;
-      if constexpr (MODE == 1) {
-        weno5_first<T, false>((T)(q0 - q2), (T)(q1 - q2), T(0), (T)(q3 - q2), (T)(q4 - q2), wm,
-                              wp);
-      } else {
-        weno5_first<T, EX>((T)q0, (T)q1, (T)q2, (T)q3, (T)q4, wm, wp);
+    if constexpr (MODE == 1) {
+      // two columns per item (packed pairs)
+      static_assert(FW % 2 == 0, "column pairs");
+      constexpr int FW2 = FW / 2;
+      for (int it = tid; it < 3 * FH * FW2; it += NT) {
+        int cp = it % FW2, rest = it / FW2, rr = rest % FH, v = rest / FH;
+        const int cc = 2 * cp;
+        // V rows (j0-1+rr)-2 .. +2 -> tile rows rr..rr+4; col (i0-2+cc) -> tile col cc+1
+        const double ca = SV(v, rr + 2, cc + 1), cb = SV(v, rr + 2, cc + 2);
+        f2 q[5];
+#pragma unroll
+        for (int k = 0; k < 5; ++k)
+          q[k] = f2_pack((float)(SV(v, rr + k, cc + 1) - ca), (float)(SV(v, rr + k, cc + 2) - cb));
+        f2 wm, wp;
+        weno5_first_x2(q[0], q[1], q[2], q[3], q[4], wm, wp);
+        f2_unpack(wm, sTM[(v * FH + rr) * FW + cc], sTM[(v * FH + rr) * FW + cc + 1]);
+        f2_unpack(wp, sTP[(v * FH + rr) * FW + cc], sTP[(v * FH + rr) * FW + cc + 1]);
       }
-      sTM[(v * FH + rr) * FW + cc] = wm;
-      sTP[(v * FH + rr) * FW + cc] = wp;
+    } else {
+      for (int it = tid; it < 3 * FH * FW; it += NT) {
+        int cc = it % FW, rest = it / FW, rr = rest % FH, v = rest / FH;
+        // V rows (j0-1+rr)-2 .. +2 -> tile rows rr..rr+4; col (i0-2+cc) -> tile col cc+1
+        double q0 = SV(v, rr, cc + 1), q1 = SV(v, rr + 1, cc + 1), q2 = SV(v, rr + 2, cc + 1),
+               q3 = SV(v, rr + 3, cc + 1), q4 = SV(v, rr + 4, cc + 1);
+        T wm, wp;
+        weno5_first<T, EX>((T)q0, (T)q1, (T)q2, (T)q3, (T)q4, wm, wp);
+        sTM[(v * FH + rr) * FW + cc] = wm;
+        sTP[(v * FH + rr) * FW + cc] = wp;
+      }
     }
     __syncthreads();
     // second sweeps along x; cells: cols i0..i0+TX-1 (cc), rows j0-1..j0+TY (rr)
@@ -243,15 +318,16 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const i
       const int gr_row = j0 - 1 + rr;
       if constexpr (MODE == 1) {
         float dm[4], dp[4];
-        T qm[5], qp[5];
+        f2 q[5], w[4];
 #pragma unroll
         for (int k = 0; k < 5; ++k) {
           T base = (T)(SV(v, rr + 2, cc + 1 + k) - Vc);
-          qm[k] = base + sTM[(v * FH + rr) * FW + cc + k];
-          qp[k] = base + sTP[(v * FH + rr) * FW + cc + k];
+          q[k] = f2_pack(base + sTM[(v * FH + rr) * FW + cc + k],
+                         base + sTP[(v * FH + rr) * FW + cc + k]);
         }
-        weno5_second<T, false>(qm[0], qm[1], qm[2], qm[3], qm[4], dm);
-        weno5_second<T, false>(qp[0], qp[1], qp[2], qp[3], qp[4], dp);
+        weno5_second_x2(q[0], q[1], q[2], q[3], q[4], w);
+#pragma unroll
+        for (int g = 0; g < 4; ++g) f2_unpack(w[g], dm[g], dp[g]);
         if (v == 0 && gr_row != ny) {
           limit_h_dev(gr, Vc, dm, dp, wmv, wpv);
         } else {
@@ -281,27 +357,22 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const i
       }
     }
     __syncthreads();
-    // Rusanov at faces f = j0 .. j0+TY (fr); below = WP(row f-1) (rr = fr), above = WM(f)
-    for (int it = tid; it < (TY + 1) * TX; it += NT) {
-      int cc = it % TX, fr = it / TX;
-      double s0 = 0.0, s1 = 0.0, s2 = 0.0;
-#pragma unroll
-      for (int g = 0; g < 4; ++g) {
-        const int L = fr * TX + cc, R = (fr + 1) * TX + cc;
-        double F0, F1, F2;
-        // normal = v (var 2), tangential = u (var 1)
-        rusanov<MODE == 1>(gr.g, sW[((1 * 3 + 0) * 4 + g) * WC + L], sW[((1 * 3 + 2) * 4 + g) * WC + L],
-                sW[((1 * 3 + 1) * 4 + g) * WC + L], sW[((0 * 3 + 0) * 4 + g) * WC + R],
-                sW[((0 * 3 + 2) * 4 + g) * WC + R], sW[((0 * 3 + 1) * 4 + g) * WC + R], F0, F1,
-                F2);
-        s0 = s0 + gr.qw[g] * F0;
-        s1 = s1 + gr.qw[g] * F2;  // hu component
-        s2 = s2 + gr.qw[g] * F1;  // hv component
-      }
+    // Rusanov at faces f = j0 .. j0+TY (fr); below = WP(row f-1) (rr = fr), above = WM(f);
+    // normal = v (var 2), tangential = u (var 1), so F2 is the hu and F1 the hv component
+    auto yface = [&](int f, int g, double& F0, double& F2, double& F1) {
+      const int cc = f % TX, fr = f / TX;
+      const int L = fr * TX + cc, R = (fr + 1) * TX + cc;
+      rusanov<MODE == 1>(gr.g, sW[((1 * 3 + 0) * 4 + g) * WC + L], sW[((1 * 3 + 2) * 4 + g) * WC + L],
+              sW[((1 * 3 + 1) * 4 + g) * WC + L], sW[((0 * 3 + 0) * 4 + g) * WC + R],
+              sW[((0 * 3 + 2) * 4 + g) * WC + R], sW[((0 * 3 + 1) * 4 + g) * WC + R], F0, F1, F2);
+    };
+    auto ystore = [&](int f, double s0, double s1, double s2) {
+      const int cc = f % TX, fr = f / TX;
       sFY[(0 * (TY + 1) + fr) * TX + cc] = s0;
       sFY[(1 * (TY + 1) + fr) * TX + cc] = s1;
       sFY[(2 * (TY + 1) + fr) * TX + cc] = s2;
-    }
+    };
+    face_pass<(TY + 1) * TX, NT>(gr, yface, ystore);
     __syncthreads();
   }
 
@@ -310,18 +381,32 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const i
   constexpr int SW_ = TX + 4;  // y-sweep columns i0-2..i0+TX+1
   T* sVt = sF1;                // [4][TY][TX+4]
   if (has_src) {
-    for (int it = tid; it < TY * SW_; it += NT) {
-      int cc = it % SW_, rr = it / SW_;
-      // U(1) = V(1) = h; rows (j0+rr)-2..+2 -> tile rows rr+1..rr+5; col i0-2+cc -> cc+1
-      double q0 = SV(0, rr + 1, cc + 1), q1 = SV(0, rr + 2, cc + 1), q2 = SV(0, rr + 3, cc + 1),
-             q3 = SV(0, rr + 4, cc + 1), q4 = SV(0, rr + 5, cc + 1);
-      T w[4];
-      if constexpr (MODE == 1)
-        weno5_second<T, false>((T)(q0 - q2), (T)(q1 - q2), T(0), (T)(q3 - q2), (T)(q4 - q2), w);
-      else
+    if constexpr (MODE == 1) {
+      static_assert(SW_ % 2 == 0, "column pairs");
+      for (int it = tid; it < TY * (SW_ / 2); it += NT) {
+        int cc = 2 * (it % (SW_ / 2)), rr = it / (SW_ / 2);
+        // U(1) = V(1) = h; rows (j0+rr)-2..+2 -> tile rows rr+1..rr+5; col i0-2+cc -> cc+1
+        const double ca = SV(0, rr + 3, cc + 1), cb = SV(0, rr + 3, cc + 2);
+        f2 q[5], w[4];
+#pragma unroll
+        for (int k = 0; k < 5; ++k)
+          q[k] = f2_pack((float)(SV(0, rr + 1 + k, cc + 1) - ca),
+                         (float)(SV(0, rr + 1 + k, cc + 2) - cb));
+        weno5_second_x2(q[0], q[1], q[2], q[3], q[4], w);
+#pragma unroll
+        for (int g = 0; g < 4; ++g)
+          f2_unpack(w[g], sVt[(g * TY + rr) * SW_ + cc], sVt[(g * TY + rr) * SW_ + cc + 1]);
+      }
+    } else {
+      for (int it = tid; it < TY * SW_; it += NT) {
+        int cc = it % SW_, rr = it / SW_;
+        double q0 = SV(0, rr + 1, cc + 1), q1 = SV(0, rr + 2, cc + 1), q2 = SV(0, rr + 3, cc + 1),
+               q3 = SV(0, rr + 4, cc + 1), q4 = SV(0, rr + 5, cc + 1);
+        T w[4];
         weno5_second<T, EX>((T)q0, (T)q1, (T)q2, (T)q3, (T)q4, w);
 #pragma unroll
-      for (int g = 0; g < 4; ++g) sVt[(g * TY + rr) * SW_ + cc] = w[g];
+        for (int g = 0; g < 4; ++g) sVt[(g * TY + rr) * SW_ + cc] = w[g];
+      }
     }
     __syncthreads();
   }
@@ -334,19 +419,32 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const i
     double S1 = 0.0, S2 = 0.0;
     if (has_src) {
       double hq[4][4];  // [x-GP a][y-GP b]
+      if constexpr (MODE == 1) {
+        const double hc = SV(0, rr + 3, cc + 3);
+        T dev[5];
 #pragma unroll
-      for (int b = 0; b < 4; ++b) {
-        const T* r = &sVt[(b * TY + rr) * SW_ + cc];
-        T w[4];
-        if constexpr (MODE == 1) {
-          const double hc = SV(0, rr + 3, cc + 3);
-          T q[5];
+        for (int k = 0; k < 5; ++k) dev[k] = (T)(SV(0, rr + 3, cc + 1 + k) - hc);
 #pragma unroll
-          for (int k = 0; k < 5; ++k) q[k] = (T)(SV(0, rr + 3, cc + 1 + k) - hc) + r[k];
-          weno5_second<T, false>(q[0], q[1], q[2], q[3], q[4], w);
+        for (int b = 0; b < 4; b += 2) {  // y-GP rows b, b+1 packed
+          const T* r0 = &sVt[(b * TY + rr) * SW_ + cc];
+          const T* r1 = &sVt[((b + 1) * TY + rr) * SW_ + cc];
+          f2 q[5], w[4];
 #pragma unroll
-          for (int aa = 0; aa < 4; ++aa) hq[aa][b] = hc + (double)w[aa];
-        } else {
+          for (int k = 0; k < 5; ++k) q[k] = f2_pack(dev[k] + r0[k], dev[k] + r1[k]);
+          weno5_second_x2(q[0], q[1], q[2], q[3], q[4], w);
+#pragma unroll
+          for (int aa = 0; aa < 4; ++aa) {
+            float lo, hi;
+            f2_unpack(w[aa], lo, hi);
+            hq[aa][b] = hc + (double)lo;
+            hq[aa][b + 1] = hc + (double)hi;
+          }
+        }
+      } else {
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+          const T* r = &sVt[(b * TY + rr) * SW_ + cc];
+          T w[4];
           weno5_second<T, EX>(r[0], r[1], r[2], r[3], r[4], w);
 #pragma unroll
           for (int aa = 0; aa < 4; ++aa) hq[aa][b] = (double)w[aa];
