@@ -203,11 +203,9 @@ cudaError_t launch_summary(const double* h, int n, double* out, cudaStream_t s) 
 // P/D entries are rebuilt from the stored mass fluxes with the same operations
 // UpdateTimeDerivative uses (finitevolume.f90:500-523).
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ double patankar_div(double prod, double h) {
-  // timediscretization.f90:913-924
-  if (h < kMinDepth) return 0.;
-  return 2. * h * prod / (h * h + dmax(h * h, kMinDepth));
-}
+// PATANKAR_DIV(p, h) = 0 if h < MIN_DEPTH, else 2 h p / den(h) with
+// den(h) = h^2 + max(h^2, MIN_DEPTH) (timediscretization.f90:913-924).
+__device__ __forceinline__ double patankar_den(double h) { return h * h + dmax(h * h, kMinDepth); }
 
 __device__ __forceinline__ double hp_read(const AssembleArgs& a, int m, int i, int j) {
   // m, i, j 0-based
@@ -222,81 +220,88 @@ __device__ __forceinline__ double hp_read(const AssembleArgs& a, int m, int i, i
   return a.hp[m][(size_t)j * a.nx + i];
 }
 
-// 2h/(h^2 + max(h^2, MIN_DEPTH)), so that PATANKAR_DIV(p, h) = p * patankar_weight(h)
-__device__ __forceinline__ double patankar_weight(double h) {
-  if (h < kMinDepth) return 0.;
-  return 2. * h / (h * h + dmax(h * h, kMinDepth));
-}
-
-template <bool FAST>
+// One cell of the combination + assembly.  Every input is loaded before any
+// arithmetic (MS stages unrolled), so all of a thread's loads are in flight together.
+//  exact: the reference's branches and operation order; each quotient correctly
+//         rounded (div_rn) from RN(1/len) and one RN(1/den(h)) per depth, i.e. equal
+//         to the division it replaces;
+//  FAST : weights w(h) = 2h/den(h) from one reciprocal per depth and P, D entries
+//         by 1/len (split and FMA forms).  For a face flux f only one of
+//         P = max(f,0)/len and D = -min(f,0)/len is non-zero; the zero one adds an
+//         exact zero, which leaves Mass/Diagonal unchanged.
+template <bool FAST, int MS>
 __device__ __forceinline__ void assemble_cell(const AssembleArgs& a, bool csr, const int i,
                                               const int j) {
   const int nx = a.nx, ny = a.ny;
-  const size_t k = (size_t)j * nx + i;
+  const size_t k = (size_t)j * nx + i, kx = (size_t)j * (nx + 1) + i;
+  const int im = i == 0 ? nx - 1 : i - 1, ip = i == nx - 1 ? 0 : i + 1;
+  const int jm = j == 0 ? ny - 1 : j - 1, jp = j == ny - 1 ? 0 : j + 1;
+  // ---- loads ----
   const double dt = *a.dt;
-  const int ms = a.msteps;
-  // explicit momentum
+  double fu[MS], fv[MS], fl[4][MS];
+#pragma unroll
+  for (int r = 0; r < MS; ++r) {
+    fu[r] = a.fu[r][k];
+    fv[r] = a.fv[r][k];
+    fl[0][r] = a.fym[r][k];        // S face, oriented into the cell
+    fl[1][r] = a.fxm[r][kx];       // W
+    fl[2][r] = -a.fxm[r][kx + 1];  // E
+    fl[3][r] = -a.fym[r][k + nx];  // N
+  }
+  const int m = a.m - 1;
+  const double hK = hp_read(a, m, i, j);
+  const double hL[4] = {hp_read(a, m, i, jm), hp_read(a, m, im, j), hp_read(a, m, ip, j),
+                        hp_read(a, m, i, jp)};
   double au = a.hu_n[k], av = a.hv_n[k];
-  for (int r = 0; r < ms; ++r) {
-    au = au + dt * a.theta[r] * a.fu[r][k];
-    av = av + dt * a.theta[r] * a.fv[r][k];
+  // ---- explicit momentum (timediscretization.f90:539-543) ----
+#pragma unroll
+  for (int r = 0; r < MS; ++r) {
+    au = au + dt * a.theta[r] * fu[r];
+    av = av + dt * a.theta[r] * fv[r];
   }
   a.hu_out[k] = au;
   a.hv_out[k] = av;
-  // Patankar weights
-  const int m = a.m - 1;
-  const double hK = hp_read(a, m, i, j);
-  const int ni[4] = {i, wrap(i - 1, nx), wrap(i + 1, nx), i};
-  const int nj[4] = {wrap(j - 1, ny), j, j, wrap(j + 1, ny)};
+  // ---- Patankar weights (timediscretization.f90:795-885) ----
   double M[4] = {0., 0., 0., 0.};
   double D = 1.;
-  // For a face flux f only one of P = max(f,0)/len and Q = -min(f,0)/len is non-zero,
-  // and PATANKAR_DIV of a zero entry is a zero that leaves Mass/Diagonal unchanged, so
-  // only the non-zero entry is formed; the non-zero updates keep the reference's order.
-  const double wK = FAST ? patankar_weight(hK) : 0.;
+  const double denK = patankar_den(hK), rdenK = __drcp_rn(denK);
+  const double wK = (FAST && hK >= kMinDepth) ? (2. * hK) * rdenK : 0.;
 #pragma unroll
   for (int nb = 0; nb < 4; ++nb) {
-    const double hL = hp_read(a, m, ni[nb], nj[nb]);
-    const double len = (nb == 0 || nb == 3) ? a.dy : a.dx;
-    const double ilen = (nb == 0 || nb == 3) ? a.inv_dy : a.inv_dx;
-    const double wL = FAST ? patankar_weight(hL) : 0.;
-    for (int r = 0; r < ms; ++r) {
-      double f;
-      if (nb == 0)
-        f = a.fym[r][(size_t)j * nx + i];
-      else if (nb == 1)
-        f = a.fxm[r][(size_t)j * (nx + 1) + i];
-      else if (nb == 2)
-        f = -a.fxm[r][(size_t)j * (nx + 1) + i + 1];
-      else
-        f = -a.fym[r][(size_t)(j + 1) * nx + i];
-      const double th = a.theta[r];
+    const bool ydir = (nb == 0 || nb == 3);
+    const double len = ydir ? a.dy : a.dx, ilen = ydir ? a.inv_dy : a.inv_dx;
+    const double h = hL[nb], denL = patankar_den(h), rdenL = __drcp_rn(denL);
+#pragma unroll
+    for (int r = 0; r < MS; ++r) {
+      const double f = fl[nb][r], th = a.theta[r];
       if (FAST) {
-        if (f > 0.) {
-          const double P = f * ilen;
-          if (th > 0.)
-            M[nb] = M[nb] - dt * th * (P * wL);
-          else
-            D = D - dt * th * (P * wK);
-        } else if (f < 0.) {
-          const double Q = -f * ilen;
-          if (th > 0.)
-            D = D + dt * th * (Q * wK);
-          else
-            M[nb] = M[nb] + dt * th * (Q * wL);
+        const double wL = h >= kMinDepth ? (2. * h) * rdenL : 0.;
+        const double c = dt * th, P = dmax(f, 0.) * ilen, Q = dmax(-f, 0.) * ilen;
+        if (th > 0.) {
+          M[nb] = M[nb] - c * (P * wL);
+          D = D + c * (Q * wK);
+        } else {
+          D = D - c * (P * wK);
+          M[nb] = M[nb] + c * (Q * wL);
         }
       } else if (f > 0.) {  // production P_KL = f/len
-        const double P = f / len;
-        if (th > 0.)
-          M[nb] = M[nb] - dt * th * (patankar_div(P, hL));
-        else
-          D = D - dt * th * (patankar_div(P, hK));
+        const double P = div_rn(f, len, ilen);
+        if (th > 0.) {
+          const double pd = h < kMinDepth ? 0. : div_rn(2. * h * P, denL, rdenL);
+          M[nb] = M[nb] - dt * th * pd;
+        } else {
+          const double pd = hK < kMinDepth ? 0. : div_rn(2. * hK * P, denK, rdenK);
+          D = D - dt * th * pd;
+        }
       } else if (f < 0.) {  // destruction D_KL = -f/len
-        const double Q = -f / len;
-        if (th > 0.)
-          D = D + dt * th * (patankar_div(Q, hK));
-        else
-          M[nb] = M[nb] + dt * th * (patankar_div(Q, hL));
+        const double Q = div_rn(-f, len, ilen);
+        if (th > 0.) {
+          const double pd = hK < kMinDepth ? 0. : div_rn(2. * hK * Q, denK, rdenK);
+          D = D + dt * th * pd;
+        } else {
+          const double pd = h < kMinDepth ? 0. : div_rn(2. * h * Q, denL, rdenL);
+          M[nb] = M[nb] + dt * th * pd;
+        }
       }
     }
   }
@@ -314,17 +319,17 @@ __device__ __forceinline__ void assemble_cell(const AssembleArgs& a, bool csr, c
     a.cW[k] = M[1];
     a.cE[k] = M[2];
     a.cN[k] = M[3];
-    a.cD[k] = FAST ? 1.0 / D : D;  // the fast stencil solver multiplies by 1/Diagonal
+    a.cD[k] = FAST ? __drcp_rn(D) : D;  // the fast stencil solver multiplies by 1/Diagonal
   }
   if (a.rhs_out) a.rhs_out[k] = hp_read(a, 0, i, j);  // rhs = hp(1,.) (timediscretization.f90:887)
 }
 
-template <bool FAST>
-__global__ void assemble_kernel(const AssembleArgs a, bool csr) {
+template <bool FAST, int MS>
+__global__ void __launch_bounds__(128) assemble_kernel(const AssembleArgs a, bool csr) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y;
   if (i >= a.nx || j >= a.ny) return;
-  assemble_cell<FAST>(a, csr, i, j);
+  assemble_cell<FAST, MS>(a, csr, i, j);
 }
 
 // Ensembles: block b covers cells [cell0, cell0+128) of problem blk[b].x, with
@@ -341,7 +346,10 @@ __global__ void __launch_bounds__(128)
   __syncthreads();
   const int c = w.y + threadIdx.x;
   if (c >= sa.nx * sa.ny) return;
-  assemble_cell<FAST>(sa, false, c % sa.nx, c / sa.nx);
+  if (sa.msteps == 4)
+    assemble_cell<FAST, 4>(sa, false, c % sa.nx, c / sa.nx);
+  else
+    assemble_cell<FAST, 2>(sa, false, c % sa.nx, c / sa.nx);
 }
 
 cudaError_t launch_assemble_batch(const AssembleArgs* descs, const int2* blk, int nblk, bool fast,
@@ -356,10 +364,18 @@ cudaError_t launch_assemble_batch(const AssembleArgs* descs, const int2* blk, in
 
 cudaError_t launch_assemble(const AssembleArgs& a, bool csr, cudaStream_t s) {
   dim3 blk(128), grd((a.nx + 127) / 128, a.ny);
-  if (a.fast && !csr)
-    assemble_kernel<true><<<grd, blk, 0, s>>>(a, csr);
-  else
-    assemble_kernel<false><<<grd, blk, 0, s>>>(a, csr);
+  const bool fast = a.fast && !csr;
+  if (a.msteps == 4) {
+    if (fast)
+      assemble_kernel<true, 4><<<grd, blk, 0, s>>>(a, csr);
+    else
+      assemble_kernel<false, 4><<<grd, blk, 0, s>>>(a, csr);
+  } else {
+    if (fast)
+      assemble_kernel<true, 2><<<grd, blk, 0, s>>>(a, csr);
+    else
+      assemble_kernel<false, 2><<<grd, blk, 0, s>>>(a, csr);
+  }
   return cudaGetLastError();
 }
 
