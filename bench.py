@@ -37,6 +37,24 @@ sys.path.insert(0, os.path.join(ROOT, "sw-mpdec_b200"))
 METRIC = "mPDeC5 cell-steps/s at 2048²: split-precision vs FP64 GPU at L1 err ≤1e-6"
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
 
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the split
+# step's kernels from one ncu capture each at 2048x2048 (4,194,304 cells); the named
+# summary under profiles/ holds the command and the counters.  Scaled by cells for
+# other grid sizes (the traffic of these kernels grows with the cell count).
+NCU_TRAFFIC_2048 = {
+    "rhs": (None, "profiles/rhs_split_island2048.md"),
+    "patankar_assemble": (None, "profiles/assemble_split_island2048.md"),
+    "jacobi": (None, "profiles/jacobi_stencil4_split_island2048.md"),
+}
+
+# Algorithmic bytes per cell-step of the whole mPDeC5 step: every phase reads its
+# inputs and writes its outputs once (halo re-reads not counted), the Patankar
+# matrix is re-read on every Jacobi sweep.  Per step: dt reduction 24, 13 RHS (FP64
+# 56 / split 40), 13 combinations (96 / 64), 13 assemblies (112 / 80), and 64 per
+# Jacobi sweep summed over the 13 solves.
+STEP_BYTES_BASE = {"fp64": 3456.0, "split": 2416.0}
+STEP_BYTES_PER_SWEEP = 64.0
+
 
 def peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -348,6 +366,16 @@ def main():
         alg = 208.0 * cells
     t_launch = classes[dom][0] / max(classes[dom][1], 1) * 1e-3
     achieved = alg / t_launch / 1e9
+    tb, traffic_src = NCU_TRAFFIC_2048.get(dom, (None, None))
+    traffic = tb * cells / 2048.0**2 if tb else None
+    # whole-step byte model for both forms (N_J = measured Jacobi sweeps per step)
+    step_rf = {"unit": "GB/s", "peak": peak, "jacobi_sweeps_per_step": nj,
+               "bytes_per_cell_step": {}, "achieved": {}, "frac": {}}
+    for form, val, sweeps in (("split", value, nj), ("fp64", value64, fp["iters"] / args.steps)):
+        b = STEP_BYTES_BASE[form] + STEP_BYTES_PER_SWEEP * sweeps
+        step_rf["bytes_per_cell_step"][form] = b
+        step_rf["achieved"][form] = val / world * b / 1e9  # per GPU (replicas)
+        step_rf["frac"][form] = val / world * b / 1e9 / peak
     launches = sum(v[1] for v in classes.values()) + 1  # + dt reduction
     line = {
         "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world,
@@ -367,8 +395,10 @@ def main():
         "jacobi_iters_per_step": nj,
         "kernel_ms_per_step": {k: v[0] for k, v in classes.items()},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
-                     "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                     "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                     "traffic_source": traffic_src, "alg_bytes_per_launch": alg,
                      "peak_source": src},
+        "step_roofline": step_rf,
         "gpu_launches": launches * args.steps,
         "clocks": clocks,
         "e2e": e2e,

@@ -67,8 +67,10 @@ struct RhsSmem {
   static constexpr int nW = 2 * 3 * 4 * (WX > WY ? WX : WY);      // double
   static constexpr int nFX = 3 * TY * (TX + 1);                   // double
   static constexpr int nFY = 3 * (TY + 1) * TX;                   // double
+  // split form: V also as float pairs hi + lo (hi = fl32(V), lo = fl32(V - hi))
+  static constexpr int nVF = std::is_same<T, float>::value ? 2 * nV : 0;  // float
   static constexpr size_t bytes =
-      sizeof(double) * (nV + nW + nFX + nFY) + sizeof(T) * nF1;
+      sizeof(double) * (nV + nW + nFX + nFY) + sizeof(T) * nF1 + sizeof(float) * nVF;
 };
 
 }  // namespace swm
@@ -143,6 +145,8 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const i
   double* sFX = sW + SM::nW;                         // [3][TY][TX+1]
   double* sFY = sFX + SM::nFX;                       // [3][TY+1][TX]
   T* sF1 = reinterpret_cast<T*>(sFY + SM::nFY);      // [2][3][...]
+  float* sVh = reinterpret_cast<float*>(sF1 + SM::nF1);  // split: [3][VY][VX] hi parts
+  float* sVl = sVh + SM::nV;                              //        and lo parts
 
   const Grid& gr = a.gr;
   const int nx = gr.nx, ny = gr.ny;
@@ -168,9 +172,25 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const i
     sV[(0 * VY + cy) * VX + cx] = h;
     sV[(1 * VY + cy) * VX + cx] = u;
     sV[(2 * VY + cy) * VX + cx] = v;
+    if constexpr (MODE == 1) {
+      const double q[3] = {h, u, v};
+#pragma unroll
+      for (int w = 0; w < 3; ++w) {
+        const float hi = (float)q[w];
+        sVh[(w * VY + cy) * VX + cx] = hi;
+        sVl[(w * VY + cy) * VX + cx] = (float)(q[w] - (double)hi);
+      }
+    }
   }
   __syncthreads();
 #define SV(v, y, x) sV[((v) * VY + (y)) * VX + (x)]
+  // split form: V(v,y,x) - V(v,yc,xc) in FP32 from the hi/lo pairs, (hi - hi_c) +
+  // (lo - lo_c): exact hi difference for values within a factor 2 (Sterbenz), else
+  // one FP32 rounding, the same accuracy as rounding the FP64 difference
+  auto dev = [&](int v, int y, int x, int yc, int xc) -> float {
+    const int k = (v * VY + y) * VX + x, kc = (v * VY + yc) * VX + xc;
+    return (sVh[k] - sVh[kc]) + (sVl[k] - sVl[kc]);
+  };
 
   // ======================= x direction =======================
   {
@@ -184,12 +204,10 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const i
       for (int it = tid; it < 3 * FH2 * FW; it += NT) {
         int cc = it % FW, rest = it / FW, rp = rest % FH2, v = rest / FH2;
         const int rr = 2 * rp;
-        const double* qa = &SV(v, rr + 1, cc);
-        const double* qb = &SV(v, rr + 2, cc);
-        const double ca = qa[2], cb = qb[2];
         f2 q[5];
 #pragma unroll
-        for (int k = 0; k < 5; ++k) q[k] = f2_pack((float)(qa[k] - ca), (float)(qb[k] - cb));
+        for (int k = 0; k < 5; ++k)
+          q[k] = f2_pack(dev(v, rr + 1, cc + k, rr + 1, cc + 2), dev(v, rr + 2, cc + k, rr + 2, cc + 2));
         f2 wm, wp;
         weno5_first_x2(q[0], q[1], q[2], q[3], q[4], wm, wp);
         f2_unpack(wm, sTM[(v * FH + rr) * FW + cc], sTM[(v * FH + rr + 1) * FW + cc]);
@@ -217,7 +235,7 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const i
         f2 q[5], w[4];
 #pragma unroll
         for (int k = 0; k < 5; ++k) {
-          T base = (T)(SV(v, rr + 1 + k, cc + 2) - Vc);  // row offset to the centre row
+          T base = dev(v, rr + 1 + k, cc + 2, rr + 3, cc + 2);  // row offset to the centre row
           q[k] = f2_pack(base + sTM[(v * FH + rr + k) * FW + cc],
                          base + sTP[(v * FH + rr + k) * FW + cc]);
         }
@@ -279,22 +297,21 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const i
     T* sTM = sF1;
     T* sTP = sF1 + 3 * FH * FW;
     if constexpr (MODE == 1) {
-      // two columns per item (packed pairs)
-      static_assert(FW % 2 == 0, "column pairs");
-      constexpr int FW2 = FW / 2;
-      for (int it = tid; it < 3 * FH * FW2; it += NT) {
-        int cp = it % FW2, rest = it / FW2, rr = rest % FH, v = rest / FH;
-        const int cc = 2 * cp;
+      // two rows per item (packed pairs): the vertical stencils of rows rr and rr+1
+      // share four of their six values
+      static_assert(FH % 2 == 0, "row pairs");
+      constexpr int FH2 = FH / 2;
+      for (int it = tid; it < 3 * FH2 * FW; it += NT) {
+        int cc = it % FW, rest = it / FW, rr = 2 * (rest % FH2), v = rest / FH2;
         // V rows (j0-1+rr)-2 .. +2 -> tile rows rr..rr+4; col (i0-2+cc) -> tile col cc+1
-        const double ca = SV(v, rr + 2, cc + 1), cb = SV(v, rr + 2, cc + 2);
         f2 q[5];
 #pragma unroll
         for (int k = 0; k < 5; ++k)
-          q[k] = f2_pack((float)(SV(v, rr + k, cc + 1) - ca), (float)(SV(v, rr + k, cc + 2) - cb));
+          q[k] = f2_pack(dev(v, rr + k, cc + 1, rr + 2, cc + 1), dev(v, rr + k + 1, cc + 1, rr + 3, cc + 1));
         f2 wm, wp;
         weno5_first_x2(q[0], q[1], q[2], q[3], q[4], wm, wp);
-        f2_unpack(wm, sTM[(v * FH + rr) * FW + cc], sTM[(v * FH + rr) * FW + cc + 1]);
-        f2_unpack(wp, sTP[(v * FH + rr) * FW + cc], sTP[(v * FH + rr) * FW + cc + 1]);
+        f2_unpack(wm, sTM[(v * FH + rr) * FW + cc], sTM[(v * FH + rr + 1) * FW + cc]);
+        f2_unpack(wp, sTP[(v * FH + rr) * FW + cc], sTP[(v * FH + rr + 1) * FW + cc]);
       }
     } else {
       for (int it = tid; it < 3 * FH * FW; it += NT) {
@@ -321,7 +338,7 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const i
         f2 q[5], w[4];
 #pragma unroll
         for (int k = 0; k < 5; ++k) {
-          T base = (T)(SV(v, rr + 2, cc + 1 + k) - Vc);
+          T base = dev(v, rr + 2, cc + 1 + k, rr + 2, cc + 3);
           q[k] = f2_pack(base + sTM[(v * FH + rr) * FW + cc + k],
                          base + sTP[(v * FH + rr) * FW + cc + k]);
         }
@@ -382,20 +399,19 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const i
   T* sVt = sF1;                // [4][TY][TX+4]
   if (has_src) {
     if constexpr (MODE == 1) {
-      static_assert(SW_ % 2 == 0, "column pairs");
-      for (int it = tid; it < TY * (SW_ / 2); it += NT) {
-        int cc = 2 * (it % (SW_ / 2)), rr = it / (SW_ / 2);
+      static_assert(TY % 2 == 0, "row pairs");
+      for (int it = tid; it < (TY / 2) * SW_; it += NT) {
+        int cc = it % SW_, rr = 2 * (it / SW_);
         // U(1) = V(1) = h; rows (j0+rr)-2..+2 -> tile rows rr+1..rr+5; col i0-2+cc -> cc+1
-        const double ca = SV(0, rr + 3, cc + 1), cb = SV(0, rr + 3, cc + 2);
         f2 q[5], w[4];
 #pragma unroll
         for (int k = 0; k < 5; ++k)
-          q[k] = f2_pack((float)(SV(0, rr + 1 + k, cc + 1) - ca),
-                         (float)(SV(0, rr + 1 + k, cc + 2) - cb));
+          q[k] = f2_pack(dev(0, rr + 1 + k, cc + 1, rr + 3, cc + 1),
+                         dev(0, rr + 2 + k, cc + 1, rr + 4, cc + 1));
         weno5_second_x2(q[0], q[1], q[2], q[3], q[4], w);
 #pragma unroll
         for (int g = 0; g < 4; ++g)
-          f2_unpack(w[g], sVt[(g * TY + rr) * SW_ + cc], sVt[(g * TY + rr) * SW_ + cc + 1]);
+          f2_unpack(w[g], sVt[(g * TY + rr) * SW_ + cc], sVt[(g * TY + rr + 1) * SW_ + cc]);
       }
     } else {
       for (int it = tid; it < TY * SW_; it += NT) {
@@ -421,16 +437,16 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const i
       double hq[4][4];  // [x-GP a][y-GP b]
       if constexpr (MODE == 1) {
         const double hc = SV(0, rr + 3, cc + 3);
-        T dev[5];
+        T dv[5];
 #pragma unroll
-        for (int k = 0; k < 5; ++k) dev[k] = (T)(SV(0, rr + 3, cc + 1 + k) - hc);
+        for (int k = 0; k < 5; ++k) dv[k] = dev(0, rr + 3, cc + 1 + k, rr + 3, cc + 3);
 #pragma unroll
         for (int b = 0; b < 4; b += 2) {  // y-GP rows b, b+1 packed
           const T* r0 = &sVt[(b * TY + rr) * SW_ + cc];
           const T* r1 = &sVt[((b + 1) * TY + rr) * SW_ + cc];
           f2 q[5], w[4];
 #pragma unroll
-          for (int k = 0; k < 5; ++k) q[k] = f2_pack(dev[k] + r0[k], dev[k] + r1[k]);
+          for (int k = 0; k < 5; ++k) q[k] = f2_pack(dv[k] + r0[k], dv[k] + r1[k]);
           weno5_second_x2(q[0], q[1], q[2], q[3], q[4], w);
 #pragma unroll
           for (int aa = 0; aa < 4; ++aa) {
