@@ -118,6 +118,28 @@ SWM_API int swm_get_planes(swm_handle h, double *planes);
  * runs one RHS on Uwb with the live kernel and precision and keeps FXWB, FYWB, SWB. */
 SWM_API int swm_set_wb_state(swm_handle h, const double *Uwb_ghosted);
 
+/* ---- driver-side initialisation and post-processing on the device ----
+ * Initial condition `ic` evaluated by ExactFunction (equation.f90:70-230) and
+ * averaged with the 4x4 Gauss rule of FillInitialConditions (finitevolume.f90:281-333):
+ *   ic 1..6   the reference's cases (1 the smooth vortex, 2 sin/cos lake, 3 and 6
+ *             perturbations over the bathymetry, 4 and 5 circular dam breaks);
+ *   ic 101    vortex            par {cx, cy, eps, ub, vb, R}
+ *   ic 102    lake + pulse      par {amp, x_lo, x_hi}   (bathymetry from the params)
+ *   ic 103    dam break         par {cx, cy, radius, h_in}
+ *   ic 104    wave over island  par {amp, xc, width}    (bathymetry from the params)
+ *   ic 105    still water       par {level}
+ * par holds npar <= 8 values (nullable when npar = 0).  Transcendental functions are
+ * CUDA's, so cell averages match a host evaluation to the last few bits. */
+/* U := the cell averages of ic (replaces CALL FillInitialConditions, main.f90:23). */
+SWM_API int swm_fill_ic(swm_handle h, int ic, const double *par, int npar);
+/* InitializeWBVariables (finitevolume.f90:339-396) from ic: the WB fluxes and source
+ * of its cell averages with the live kernel; the state is left unchanged. */
+SWM_API int swm_init_wb_ic(swm_handle h, int ic, const double *par, int npar);
+/* PostProcessing (postprocessing.f90:23-60): l1[v] = sum_cells |U - Uexact(ic, t)| dx dy
+ * for v = h, hu, hv (case 1 is advected to time t; the others do not depend on t). */
+SWM_API int swm_l1_error(swm_handle h, int ic, const double *par, int npar, double t,
+                         double l1[3]);
+
 /* TimeStep() (equation.f90:791-837): CFL time step of the current state. */
 SWM_API int swm_timestep(swm_handle h, double *dt_min);
 

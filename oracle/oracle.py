@@ -48,6 +48,7 @@ def _lib(threaded=False):
     lib.orc_fill_ic.argtypes = [ctypes.c_void_p, ctypes.c_int, dp]
     lib.orc_init_wb.argtypes = [ctypes.c_void_p, ctypes.c_int, dp]
     lib.orc_init_wb_planes.argtypes = [ctypes.c_void_p, dp]
+    lib.orc_l1_error.argtypes = [ctypes.c_void_p, ctypes.c_int, dp, ctypes.c_double, dp]
     lib.orc_set_state.argtypes = [ctypes.c_void_p, dp]
     lib.orc_get_state.argtypes = [ctypes.c_void_p, dp, dp]
     lib.orc_get_planes.argtypes = [ctypes.c_void_p, dp]
@@ -132,6 +133,15 @@ class Oracle:
         par = np.ascontiguousarray(np.array(list(par) + [0.0] * 8, dtype=np.float64))
         if self.lib.orc_init_wb(self.h, ic, _dp(par)) != 0:
             raise ValueError(f"unknown WB condition {ic}")
+
+    def l1_error(self, ic, par=(), t=0.0):
+        """PostProcessing (postprocessing.f90:23-60): per-variable L1 error of the state
+        against the exact solution of `ic` at time t, times dx dy."""
+        par = np.ascontiguousarray(np.array(list(par) + [0.0] * 8, dtype=np.float64))
+        out = np.zeros(3)
+        if self.lib.orc_l1_error(self.h, ic, _dp(par), float(t), _dp(out)) != 0:
+            raise ValueError(f"unknown initial condition {ic}")
+        return out
 
     def init_wb_planes(self, planes):
         planes = np.ascontiguousarray(planes, dtype=np.float64)

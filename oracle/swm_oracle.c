@@ -858,9 +858,10 @@ int orc_run(orc_t *o, double tend, int n_outputs, double *t_out) {
 /* Fortran MODULO for reals */
 static inline double rmodulo(double a, double p) { return a - floor(a / p) * p; }
 
-/* equation.f90:70-230 ExactFunction at t = 0, plus the new benchmark cases. */
-static void exact_function(const orc_t *o, int ic, const double *par, double x, double y,
-                           double cons[3]) {
+/* equation.f90:70-230 ExactFunction at time t (only case 1, the vortex advected by
+ * (u_inf, v_inf), depends on t), plus the new benchmark cases. */
+static void exact_function(const orc_t *o, int ic, const double *par, double t, double x,
+                           double y, double cons[3]) {
   const double PI = acos(-1.0);
   const double g = o->p.g;
   double prim[3] = {0., 0., 0.};
@@ -869,8 +870,8 @@ static void exact_function(const orc_t *o, int ic, const double *par, double x, 
     case 1: { /* unsteady smooth vortex */
       double u_inf = 2., v_inf = 3., H_inf = 1.;
       double xm0 = o->p.x0[0] + 0.5 * o->sx[0], xm1 = o->p.x0[1] + 0.5 * o->sx[1];
-      double xc0 = rmodulo(x - u_inf * 0.0 - o->p.x0[0], o->sx[0]) + o->p.x0[0] - xm0;
-      double xc1 = rmodulo(y - v_inf * 0.0 - o->p.x0[1], o->sx[1]) + o->p.x0[1] - xm1;
+      double xc0 = rmodulo(x - u_inf * t - o->p.x0[0], o->sx[0]) + o->p.x0[0] - xm0;
+      double xc1 = rmodulo(y - v_inf * t - o->p.x0[1], o->sx[1]) + o->p.x0[1] - xm1;
       double r = xc0 * xc0 + xc1 * xc1;
       prim[0] = H_inf;
       prim[1] = u_inf;
@@ -960,10 +961,30 @@ int orc_fill_ic(orc_t *o, int ic, const double *par) {
       for (int iGP = 0; iGP < 4; ++iGP)
         for (int jGP = 0; jGP < 4; ++jGP) {
           double ut[3];
-          exact_function(o, ic, par, gp_coord(o, 0, ii, iGP), gp_coord(o, 1, jj, jGP), ut);
+          exact_function(o, ic, par, 0.0, gp_coord(o, 0, ii, iGP), gp_coord(o, 1, jj, jGP), ut);
           for (int v = 0; v < 3; ++v)
             o->U[IU(v, ii, jj)] = o->U[IU(v, ii, jj)] + o->wgp[iGP][jGP] * ut[v];
         }
+  return 0;
+}
+
+/* postprocessing.f90:23-60 PostProcessing: L1error(v) = sum_cells |U - Uexact(t)| dx dy,
+ * Uexact the 4x4 Gauss average of ExactFunction(ic, t) (serial sum, cell order j, i). */
+int orc_l1_error(const orc_t *o, int ic, const double *par, double t, double out[3]) {
+  if (!valid_ic(ic)) return -1;
+  double l1[3] = {0., 0., 0.};
+  for (int jj = 1; jj <= NY; ++jj)
+    for (int ii = 1; ii <= NX; ++ii) {
+      double ue[3] = {0., 0., 0.};
+      for (int iGP = 0; iGP < 4; ++iGP)
+        for (int jGP = 0; jGP < 4; ++jGP) {
+          double ut[3];
+          exact_function(o, ic, par, t, gp_coord(o, 0, ii, iGP), gp_coord(o, 1, jj, jGP), ut);
+          for (int v = 0; v < 3; ++v) ue[v] = ue[v] + o->wgp[iGP][jGP] * ut[v];
+        }
+      for (int v = 0; v < 3; ++v) l1[v] = l1[v] + fabs(o->U[IU(v, ii, jj)] - ue[v]);
+    }
+  for (int v = 0; v < 3; ++v) out[v] = l1[v] * o->dx[0] * o->dx[1];
   return 0;
 }
 

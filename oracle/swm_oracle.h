@@ -68,6 +68,9 @@ int orc_fill_ic(orc_t *o, int ic, const double *par);
 int orc_init_wb(orc_t *o, int ic, const double *par);
 /* The same from given cell averages [3][ny][nx]. */
 int orc_init_wb_planes(orc_t *o, const double *planes);
+/* PostProcessing (postprocessing.f90:23-60): L1 error of U against the Gauss average
+ * of ExactFunction(ic, t) (case 1 advected to time t), times dx dy, per variable. */
+int orc_l1_error(const orc_t *o, int ic, const double *par, double t, double out[3]);
 
 /* Ghosted state (3, nx+6, ny+6), var fastest (Fortran U(1:3,-2:nx+3,-2:ny+3)). */
 void orc_set_state(orc_t *o, const double *U);

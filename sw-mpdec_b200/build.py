@@ -6,6 +6,8 @@ Translation units and their floating-point flags:
   swm_rhs_fast.cu   default      (RHS, FP64 with contraction and the split form)
   swm_capi.cu       host orchestration, C ABI
   swm_batch.cu      batched ensembles
+  swm_noalloc.cu    allocation-free Jacobi entry point
+  swm_ic.cu         -fmad=false  (initial conditions, L1 error)
 Usage: python sw-mpdec_b200/build.py [--verbose] [--force]
 """
 import os
@@ -27,6 +29,7 @@ UNITS = [
     ("swm_capi.cu", ["-Xcompiler", "-ffp-contract=off"]),
     ("swm_batch.cu", []),
     ("swm_noalloc.cu", []),
+    ("swm_ic.cu", ["-fmad=false"]),
 ]
 
 

@@ -87,6 +87,7 @@ struct swm_solver {
   int* bad = nullptr;
   JacobiCtl* ctl = nullptr;
   double* summary = nullptr;
+  double* l1_scratch = nullptr;  // L1 error: 3 * kIcMaxBlocks partials + 3 results
   double* stage = nullptr;  // ghosted staging (3*(nx+6)*(ny+6))
   double* stage2 = nullptr;
   // pinned host mirrors
@@ -561,6 +562,74 @@ int swm_get_planes(swm_handle s, double* P) {
   CK(cudaMemcpyAsync(P, s->h, s->N * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
   CK(cudaMemcpyAsync(P + s->N, s->hu, s->N * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
   CK(cudaMemcpyAsync(P + 2 * s->N, s->hv, s->N * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return SWM_OK;
+}
+
+// Initial condition / exact solution arguments for planes (h, hu, hv).
+static int make_ic_args(swm_solver* s, int ic, const double* par, int npar, double t, double* h,
+                        double* hu, double* hv, IcArgs* a) {
+  if (!ic_supported(ic)) return fail(SWM_ERR_PARAM, "unknown initial condition");
+  if (npar < 0 || npar > 8 || (npar > 0 && !par))
+    return fail(SWM_ERR_PARAM, "npar must be 0..8 with a parameter array");
+  *a = IcArgs{};
+  a->gr = s->gr;
+  a->ic = ic;
+  for (int k = 0; k < npar; ++k) a->par[k] = par[k];
+  a->t = t;
+  a->sx[0] = fabs(s->p.x1[0] - s->p.x0[0]);
+  a->sx[1] = fabs(s->p.x1[1] - s->p.x0[1]);
+  a->h = h;
+  a->hu = hu;
+  a->hv = hv;
+  return SWM_OK;
+}
+
+int swm_fill_ic(swm_handle s, int ic, const double* par, int npar) {
+  if (!s) return fail(SWM_ERR_PARAM, "null handle");
+  IcArgs a;
+  int rc = make_ic_args(s, ic, par, npar, 0.0, s->h, s->hu, s->hv, &a);
+  if (rc) return rc;
+  CK(cudaSetDevice(s->device));
+  CK(launch_ic_fill(a, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  s->have_state = true;
+  return SWM_OK;
+}
+
+int swm_init_wb_ic(swm_handle s, int ic, const double* par, int npar) {
+  if (!s) return fail(SWM_ERR_PARAM, "null handle");
+  if (!s->p.well_balanced) return fail(SWM_ERR_STATE, "handle created without well_balanced");
+  // scratch planes: substep-2 buffers are free between steps
+  double *h = s->hbuf[1][0], *hu = s->hum[1], *hv = s->hvm[1];
+  IcArgs ia;
+  int rc = make_ic_args(s, ic, par, npar, 0.0, h, hu, hv, &ia);
+  if (rc) return rc;
+  CK(cudaSetDevice(s->device));
+  CK(launch_ic_fill(ia, s->stream));
+  RhsArgs a = make_rhs_args(s, h, hu, hv, 1);
+  a.fx_wb = a.fy_wb = a.s_wb = nullptr;  // FXWB = 0 during InitializeWBVariables
+  a.fx_full = s->fxwb;
+  a.fy_full = s->fywb;
+  a.s_full = s->swb;
+  CK(launch_rhs(s, a));
+  CK(cudaStreamSynchronize(s->stream));
+  s->have_wb = true;
+  drop_graph(s);  // the step graph bakes the WB pointers in
+  return SWM_OK;
+}
+
+int swm_l1_error(swm_handle s, int ic, const double* par, int npar, double t, double l1[3]) {
+  if (!s || !l1) return fail(SWM_ERR_PARAM, "null argument");
+  if (!s->have_state) return fail(SWM_ERR_STATE, "no state set");
+  IcArgs a;
+  int rc = make_ic_args(s, ic, par, npar, t, s->h, s->hu, s->hv, &a);
+  if (rc) return rc;
+  CK(cudaSetDevice(s->device));
+  if (!s->l1_scratch && (rc = s->dalloc(&s->l1_scratch, 3 * (size_t)kIcMaxBlocks + 3))) return rc;
+  double* out = s->l1_scratch + 3 * kIcMaxBlocks;
+  CK(launch_l1_error(a, s->l1_scratch, out, s->stream));
+  CK(cudaMemcpyAsync(l1, out, 3 * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
   CK(cudaStreamSynchronize(s->stream));
   return SWM_OK;
 }

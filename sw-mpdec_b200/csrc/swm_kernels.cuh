@@ -156,6 +156,24 @@ cudaError_t launch_ghosted_to_planes(const double* G, int nx, int ny, double* h,
 cudaError_t launch_planes_to_ghosted(const double* h, const double* hu, const double* hv, int nx,
                                      int ny, double* G, double* Vg, cudaStream_t s);
 cudaError_t launch_summary(const double* h, int n, double* out /*[2]*/, cudaStream_t s);
+
+// Initial conditions and the L1 error on the device (swm_ic.cu).
+struct IcArgs {
+  Grid gr;
+  int ic;            // ExactFunction case: 1..6 (equation.f90:109-206), 101..105
+  double par[8];     // parameters of cases 101..105
+  double t;          // time of the exact solution (case 1 is advected)
+  double sx[2];      // domain extents |x1 - x0| (MESH_SX)
+  double* h;         // planes [ny][nx]: written by the fill, read by the L1 error
+  double* hu;
+  double* hv;
+};
+constexpr int kIcMaxBlocks = 148 * 8;
+bool ic_supported(int ic);
+int ic_blocks(int ncells);
+cudaError_t launch_ic_fill(const IcArgs& a, cudaStream_t s);
+// partial: 3 * ic_blocks(nx*ny) doubles of scratch; out: 3 doubles (device)
+cudaError_t launch_l1_error(const IcArgs& a, double* partial, double* out, cudaStream_t s);
 void residual_limbs_host(double v, unsigned long long out[3]);
 
 }  // namespace swm

@@ -28,6 +28,7 @@ EXPORTS = [
     "swm_get_stream", "swm_profile_step", "swm_debug_rhs", "swm_debug_jacobi", "swm_batch_create", "swm_batch_destroy",
     "swm_batch_set_planes", "swm_batch_get_planes", "swm_batch_step", "swm_batch_cells",
     "swm_jacobi_noalloc", "swm_batch_get_stats", "swm_batch_get_stream",
+    "swm_fill_ic", "swm_init_wb_ic", "swm_l1_error",
 ]
 
 
@@ -83,6 +84,9 @@ def load():
     lib.swm_set_planes.argtypes = [vp, dp]
     lib.swm_get_planes.argtypes = [vp, dp]
     lib.swm_set_wb_state.argtypes = [vp, dp]
+    lib.swm_fill_ic.argtypes = [vp, ctypes.c_int, dp, ctypes.c_int]
+    lib.swm_init_wb_ic.argtypes = [vp, ctypes.c_int, dp, ctypes.c_int]
+    lib.swm_l1_error.argtypes = [vp, ctypes.c_int, dp, ctypes.c_int, ctypes.c_double, dp]
     lib.swm_timestep.argtypes = [vp, dp]
     lib.swm_step.argtypes = [vp, ctypes.c_double, ctypes.c_double]
     lib.swm_run.argtypes = [vp, ctypes.c_double, ctypes.c_int, P(ctypes.c_int), dp]
@@ -190,6 +194,28 @@ class Solver:
     def set_wb_state(self, Uwb):
         Uwb = np.ascontiguousarray(Uwb, dtype=np.float64)
         _check(self.lib.swm_set_wb_state(self.h, _dp(Uwb)))
+
+    @staticmethod
+    def _par(par):
+        par = np.ascontiguousarray(np.array(list(par) if par is not None else [], dtype=np.float64))
+        return (_dp(par) if par.size else None), int(par.size), par
+
+    def fill_ic(self, ic, par=()):
+        """U := 4x4 Gauss averages of ExactFunction case `ic` (FillInitialConditions)."""
+        p, n, keep = self._par(par)
+        _check(self.lib.swm_fill_ic(self.h, int(ic), p, n))
+
+    def init_wb_ic(self, ic, par=()):
+        """InitializeWBVariables from case `ic` evaluated on the device."""
+        p, n, keep = self._par(par)
+        _check(self.lib.swm_init_wb_ic(self.h, int(ic), p, n))
+
+    def l1_error(self, ic, par=(), t=0.0):
+        """PostProcessing: per-variable L1 error against ExactFunction(ic, t), times dx dy."""
+        p, n, keep = self._par(par)
+        out = np.zeros(3)
+        _check(self.lib.swm_l1_error(self.h, int(ic), p, n, float(t), _dp(out)))
+        return out
 
     def timestep(self):
         dt = ctypes.c_double()

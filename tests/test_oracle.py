@@ -203,3 +203,26 @@ def test_mpdec2_runs_and_compat_differs():
         outs.append(o.get_planes())
     assert np.all(np.isfinite(outs[0]))
     assert not np.array_equal(outs[0], outs[1], equal_nan=True)
+
+
+def test_l1_error_postprocessing():
+    # PostProcessing (postprocessing.f90:23-60): zero on the exact cell averages, and a
+    # perturbation delta of one cell shows up as delta * dx * dy
+    c = cases.case("vortex", n=24)
+    o = O.Oracle(O.make_params(c["nx"], c["ny"], c["x0"], c["x1"], g=c["g"], cfl=c["cfl"]))
+    o.fill_ic(c["ic"], c["par"])
+    assert np.array_equal(o.l1_error(c["ic"], c["par"]), np.zeros(3))
+    P = o.get_planes()
+    P[1, 3, 5] += 0.25
+    o.set_planes(P)
+    dx = (c["x1"][0] - c["x0"][0]) / c["nx"]
+    dy = (c["x1"][1] - c["x0"][1]) / c["ny"]
+    l1 = o.l1_error(c["ic"], c["par"])
+    assert l1[0] == 0.0 and l1[2] == 0.0
+    assert abs(l1[1] - 0.25 * dx * dy) <= 1e-15
+    # the reference vortex (case 1) moves with (2, 3): at t = sx/2 it is displaced
+    r = O.Oracle(O.make_params(32, 32, (0.0, 0.0), (4.0, 4.0)))
+    r.fill_ic(1)
+    assert np.all(r.l1_error(1, t=0.0) == 0.0)
+    assert r.l1_error(1, t=0.5)[0] > 1e-3
+    assert np.allclose(r.l1_error(1, t=4.0 / 2.0 * 2), 0.0, atol=1e-12)  # period 4 in x and y
