@@ -69,7 +69,11 @@ typedef struct swm_params {
   double x0[2], x1[2];   /* MESH_X0, MESH_X1 */
   double g;              /* Gravity */
   double cfl;            /* CFL (parameters.f90:139) */
-  int timescheme;        /* 5 = mPDeC5, 7 = mPDeC2 (parameters.f90:144) */
+  int timescheme;        /* parameters.f90:144 (timediscretization.f90:60-79):
+                          * 5 mPDeC5, 7 mPDeC2, 6 mPEuler (Patankar, h >= 0);
+                          * 1 forward Euler, 2 SSPRK(5,4), 3 RK65, 4 DeC5 (explicit,
+                          * as the reference built without -DPATANKAR: Ut(1) from the
+                          * mass fluxes) */
   int bathy_flag;        /* BathymetryFlag */
   double bathy_par[5];   /* SWM_BATHY_GAUSS parameters */
   int well_balanced;     /* -DWELLBALANCED (src/makefile:48) */
@@ -78,7 +82,7 @@ typedef struct swm_params {
   int jacobi_maxiter;    /* maxIter = 1000 (jacobi_iteration.f90:64) */
   double jacobi_tol;     /* tolerance = 1e-16 (jacobi_iteration.f90:63) */
   int jacobi_block;      /* stencil solver: Jacobi sweeps per pass (1..8), 0 = auto */
-  int mpdec2_compat;     /* 1: reproduce mPDeC2's hp(2,nx,ny) read of Up(:,1,:,:) */
+  int mpdec2_compat;     /* 1: reproduce the hp(2,nx,ny) read of Up(:,1,:,:) of mPDeC2 and mPEuler */
   int use_graph;         /* capture each step into a CUDA graph (1 = default) */
   int device;            /* CUDA device ordinal */
 } swm_params;
@@ -171,7 +175,8 @@ SWM_API const char *swm_strerror(int status);
 /* ---- diagnostics (parity tests) ---- */
 /* One RHS (FVTimeDerivative, finitevolume.f90:402-540) of the ghosted input
  * state.  Outputs (nullable, column-major like the reference):
- * Ut(3,nx,ny) [only Ut(2:3) computed, Ut(1)=0 as in the PATANKAR build],
+ * Ut(3,nx,ny) [Ut(1) as the build without PATANKAR forms it (finitevolume.f90:530-533);
+ * the Patankar schemes use Ut(2:3) and the mass fluxes only],
  * FX(3,0:nx,1:ny), FY(3,1:nx,0:ny), S(3,nx,ny): WB-subtracted when WB is on. */
 SWM_API int swm_debug_rhs(swm_handle h, const double *U_ghosted, double *Ut, double *FX, double *FY,
                   double *S);

@@ -51,6 +51,7 @@ struct orc {
   int *RowStart, *Cols, *SIM;
   double *Vtemp;           /* (4,-2:nx+3,1:ny), depth only */
   double *mass, *diag, *rhs, *havec, *solp, *hpk;
+  double *EK; /* explicit schemes: 8 stage arrays (3,1:nx,1:ny) */
   double dt;
   int iters[64];
   int nsolves;
@@ -285,7 +286,8 @@ orc_t *orc_create(const orc_params *p) {
   o->havec = dalloc(N);
   o->solp = dalloc(N);
   o->hpk = dalloc(4 * N);
-  if (!o->U || !o->V || !o->WM || !o->WP || !o->FX || !o->FY || !o->FluxX || !o->FluxY ||
+  o->EK = dalloc(24 * N);
+  if (!o->EK || !o->U || !o->V || !o->WM || !o->WP || !o->FX || !o->FY || !o->FluxX || !o->FluxY ||
       !o->S || !o->Ut || !o->FXWB || !o->FYWB || !o->SWB || !o->Ua || !o->Up || !o->FUp ||
       !o->Prod || !o->Dest || !o->ProdUp || !o->DestUp || !o->RowStart || !o->Cols || !o->SIM ||
       !o->Vtemp || !o->mass || !o->diag || !o->rhs || !o->havec || !o->solp || !o->hpk) {
@@ -324,7 +326,7 @@ void orc_destroy(orc_t *o) {
   double **arrs[] = {&o->U, &o->V, &o->WM, &o->WP, &o->FX, &o->FY, &o->FluxX, &o->FluxY,
                      &o->S, &o->Ut, &o->FXWB, &o->FYWB, &o->SWB, &o->Ua, &o->Up, &o->FUp,
                      &o->Prod, &o->Dest, &o->ProdUp, &o->DestUp, &o->Vtemp, &o->mass,
-                     &o->diag, &o->rhs, &o->havec, &o->solp, &o->hpk};
+                     &o->diag, &o->rhs, &o->havec, &o->solp, &o->hpk, &o->EK};
   for (size_t k = 0; k < sizeof(arrs) / sizeof(arrs[0]); ++k) free(*arrs[k]);
   free(o->RowStart);
   free(o->Cols);
@@ -602,7 +604,9 @@ static void update_time_derivative(orc_t *o, int wb) {
       f = -o->FY[IFY(0, ii, jj)];
       o->Prod[isv + 4] = fmax2(f, 0.) / dy;
       o->Dest[isv + 4] = -fmin2(f, 0.) / dy;
-      for (int v = 1; v < 3; ++v)
+      /* Ut(2:3) in the PATANKAR build; Ut(1) as the build without it computes
+       * (finitevolume.f90:530-533), used by the explicit schemes only */
+      for (int v = 0; v < 3; ++v)
         o->Ut[IC3(v, ii, jj)] = o->S[IC3(v, ii, jj)] -
                                 (o->FX[IFX(v, ii, jj)] - o->FX[IFX(v, ii - 1, jj)]) / dx -
                                 (o->FY[IFY(v, ii, jj)] - o->FY[IFY(v, ii, jj - 1)]) / dy;
@@ -767,16 +771,20 @@ static void load_state_from_ua(orc_t *o, int m) {
       for (int v = 0; v < 3; ++v) o->U[IU(v, ii, jj)] = o->Ua[I4(m, v, ii, jj)];
 }
 
-/* timediscretization.f90:458-566 (MSteps=4,KCorr=5) and :571-664 (MSteps=2,KCorr=2) */
+static int explicit_step(orc_t *o, double dt);
+
+/* timediscretization.f90:458-566 (mPDeC5: MSteps=4, KCorr=5), :571-664 (mPDeC2:
+ * MSteps=2, KCorr=2), :671-764 (mPEuler: MSteps=2, KCorr=1); schemes 1-4 below. */
 int orc_step(orc_t *o, double t, double dt) {
   (void)t; /* stage times are unused by the periodic BC and the source term */
+  if (o->p.timescheme >= 1 && o->p.timescheme <= 4) return explicit_step(o, dt);
   const int nx = NX, ny = NY;
   int msteps, kcorr;
   double theta[16];
   memset(theta, 0, sizeof(theta));
-  if (o->p.timescheme == 7) {
+  if (o->p.timescheme == 7 || o->p.timescheme == 6) {
     msteps = 2;
-    kcorr = 2;
+    kcorr = o->p.timescheme == 7 ? 2 : 1;
     theta[1 * 4 + 0] = 0.5; /* thetaDeC(2,1) */
     theta[1 * 4 + 1] = 0.5; /* thetaDeC(2,2) */
   } else {
@@ -824,6 +832,134 @@ int orc_step(orc_t *o, double t, double dt) {
   for (int s = 0; s < o->nsolves && s < 64; ++s)
     if (o->iters[s] >= o->p.jacobi_maxiter) warn = 1;
   return warn;
+}
+
+/* ---- explicit schemes (build without PATANKAR: Ut(1) from the mass fluxes) ---- */
+static double *ek(orc_t *o, int k) { return o->EK + (size_t)k * 3 * o->N; }
+
+static void copy_state_out(const orc_t *o, double *X) {
+  for (int jj = 1; jj <= NY; ++jj)
+    for (int ii = 1; ii <= NX; ++ii)
+      for (int v = 0; v < 3; ++v) X[IC3(v, ii, jj)] = o->U[IU(v, ii, jj)];
+}
+static void copy_state_in(orc_t *o, const double *X) {
+  for (int jj = 1; jj <= NY; ++jj)
+    for (int ii = 1; ii <= NX; ++ii)
+      for (int v = 0; v < 3; ++v) o->U[IU(v, ii, jj)] = X[IC3(v, ii, jj)];
+}
+
+/* TimeDiscretizationByForwardEuler :200-242, BySSPRK4 :104-195, ByRK65 :247-348,
+ * ByDeC5 :353-451, each expression in the reference's evaluation order. */
+static int explicit_step(orc_t *o, double dt) {
+  const int wb = o->p.well_balanced && o->have_wb;
+  const size_t n3 = (size_t)3 * o->N;
+  const double *Ut = o->Ut;
+  o->dt = dt;
+  o->nsolves = 0;
+  switch (o->p.timescheme) {
+    case 1: { /* U = K0 + Ut dt */
+      double *K0 = ek(o, 0);
+      copy_state_out(o, K0);
+      fv_time_derivative(o, wb);
+      for (size_t k = 0; k < n3; ++k) K0[k] = K0[k] + Ut[k] * dt;
+      copy_state_in(o, K0);
+    } break;
+    case 2: { /* SSPRK(5,4) */
+      double *K0 = ek(o, 0), *K1 = ek(o, 1), *K2 = ek(o, 2), *K3 = ek(o, 3), *K4 = ek(o, 4),
+             *K5 = ek(o, 5);
+      copy_state_out(o, K0);
+      fv_time_derivative(o, wb);
+      for (size_t k = 0; k < n3; ++k)
+        K1[k] = 1.00000000000000 * K0[k] + 0.39175222700392 * Ut[k] * dt;
+      copy_state_in(o, K1);
+      fv_time_derivative(o, wb);
+      for (size_t k = 0; k < n3; ++k)
+        K2[k] = 0.44437049406734 * K0[k] + 0.55562950593266 * K1[k] +
+                0.36841059262959 * Ut[k] * dt;
+      copy_state_in(o, K2);
+      fv_time_derivative(o, wb);
+      for (size_t k = 0; k < n3; ++k)
+        K3[k] = 0.62010185138540 * K0[k] + 0.37989814861460 * K2[k] +
+                0.25189177424738 * Ut[k] * dt;
+      copy_state_in(o, K3);
+      fv_time_derivative(o, wb);
+      for (size_t k = 0; k < n3; ++k) {
+        K4[k] = 0.17807995410773 * K0[k] + 0.82192004589227 * K3[k] +
+                0.54497475021237 * Ut[k] * dt;
+        K5[k] = Ut[k];
+      }
+      copy_state_in(o, K4);
+      fv_time_derivative(o, wb);
+      double *Un = ek(o, 6);
+      for (size_t k = 0; k < n3; ++k)
+        Un[k] = 0.00683325884039 * K0[k] + 0.51723167208978 * K2[k] + 0.12759831133288 * K3[k] +
+                0.34833675773694 * K4[k] + 0.08460416338212 * K5[k] * dt +
+                0.22600748319395 * Ut[k] * dt;
+      copy_state_in(o, Un);
+    } break;
+    case 3: { /* RK65: ARK(6,5) column-major, bRK, cRK */
+      static const double A[6][5] = {{0., 0., 0., 0., 0.},
+                                     {0.25, 0., 0., 0., 0.},
+                                     {0.125, 0.125, 0., 0., 0.},
+                                     {0., 0., 0.5, 0., 0.},
+                                     {0.1875, -0.375, 0.375, 0.5625, 0.},
+                                     {-0.42857142857142855, 1.1428571428571428, 0.8571428571428571,
+                                      -1.7142857142857142, 1.1428571428571428}};
+      static const double b[6] = {0.077777777777777778, 0., 0.35555555555555556,
+                                  0.13333333333333333, 0.35555555555555556, 0.077777777777777778};
+      double *UN0 = ek(o, 6), *St = ek(o, 7);
+      copy_state_out(o, UN0);
+      fv_time_derivative(o, wb);
+      memcpy(ek(o, 0), Ut, sizeof(double) * n3);
+      for (int st = 1; st <= 5; ++st) { /* stage st uses K0..K(st-1) */
+        for (size_t k = 0; k < n3; ++k) {
+          double acc = A[st][0] * ek(o, 0)[k];
+          for (int j = 1; j < st; ++j) acc = acc + A[st][j] * ek(o, j)[k];
+          St[k] = UN0[k] + acc * dt;
+        }
+        copy_state_in(o, St);
+        fv_time_derivative(o, wb);
+        memcpy(ek(o, st), Ut, sizeof(double) * n3);
+      }
+      for (size_t k = 0; k < n3; ++k) {
+        double acc = b[0] * ek(o, 0)[k];
+        for (int j = 1; j < 6; ++j) acc = acc + b[j] * ek(o, j)[k];
+        St[k] = UN0[k] + acc * dt;
+      }
+      copy_state_in(o, St);
+    } break;
+    case 4: { /* DeC5: MSteps 4, KCorr 5, the mPDeC5 theta table */
+      double theta[16], beta[4];
+      orc_theta_mpdec5(theta, beta);
+      /* Ua(m) in ek(m-1), FUp(m) in o->FUp-like storage ek(4..7) */
+      for (int m = 0; m < 4; ++m) copy_state_out(o, ek(o, m));
+      fv_time_derivative(o, wb);
+      for (int m = 0; m < 4; ++m) memcpy(ek(o, 4 + m), Ut, sizeof(double) * n3);
+      for (int kk = 1; kk <= 5; ++kk) {
+        const int mlo = (kk == 5) ? 4 : 2;
+        for (int ii = mlo; ii <= 4; ++ii) {
+          double *Ua = ek(o, ii - 1);
+          const double *U1 = ek(o, 0);
+          for (size_t k = 0; k < n3; ++k) {
+            double acc = U1[k];
+            for (int jj = 1; jj <= 4; ++jj)
+              acc = acc + dt * theta[(ii - 1) * 4 + (jj - 1)] * ek(o, 3 + jj)[k];
+            Ua[k] = acc;
+          }
+        }
+        if (kk != 5)
+          for (int ii = 2; ii <= 4; ++ii) {
+            copy_state_in(o, ek(o, ii - 1));
+            fv_time_derivative(o, wb);
+            memcpy(ek(o, 3 + ii), Ut, sizeof(double) * n3);
+          }
+      }
+      copy_state_in(o, ek(o, 3));
+    } break;
+    default:
+      return -1;
+  }
+  return 0;
 }
 
 /* timediscretization.f90:46-95 without output */

@@ -42,7 +42,7 @@ typedef struct orc_params {
   int nx, ny;
   double x0[2], x1[2];
   double g, cfl;
-  int timescheme;       /* 5 = mPDeC5, 7 = mPDeC2 */
+  int timescheme;       /* 1 FE, 2 SSPRK(5,4), 3 RK65, 4 DeC5, 5 mPDeC5, 6 mPEuler, 7 mPDeC2 */
   int bathy_flag;
   double bathy_par[5];
   int well_balanced;

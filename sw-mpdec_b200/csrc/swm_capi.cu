@@ -5,7 +5,10 @@
 // state lives on the device as three planes [ny][nx]; one step is the fixed
 // sequence of kernels below, captured once into a CUDA graph (dt is read from
 // device memory, so the graph is replayed unchanged every step).
+#include <array>
 #include <cmath>
+#include <initializer_list>
+#include <utility>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -88,6 +91,7 @@ struct swm_solver {
   JacobiCtl* ctl = nullptr;
   double* summary = nullptr;
   double* l1_scratch = nullptr;  // L1 error: 3 * kIcMaxBlocks partials + 3 results
+  double* ex[7][3] = {};          // explicit schemes: 7 stage slots of (h, hu, hv) planes
   double* stage = nullptr;  // ghosted staging (3*(nx+6)*(ny+6))
   double* stage2 = nullptr;
   // pinned host mirrors
@@ -124,8 +128,10 @@ static int valid_params(const swm_params* p) {
   if (!p) return fail(SWM_ERR_PARAM, "null params");
   if (p->nx < 3 || p->ny < 3) return fail(SWM_ERR_PARAM, "nx, ny must be >= 3");
   if ((long long)p->nx * p->ny > (1LL << 28)) return fail(SWM_ERR_PARAM, "grid too large");
-  if (p->timescheme != 5 && p->timescheme != 7)
-    return fail(SWM_ERR_PARAM, "timescheme must be 5 (mPDeC5) or 7 (mPDeC2)");
+  if (p->timescheme < 1 || p->timescheme > 7)
+    return fail(SWM_ERR_PARAM,
+                "timescheme must be 1 (Euler), 2 (SSPRK4), 3 (RK65), 4 (DeC5), 5 (mPDeC5), "
+                "6 (mPEuler) or 7 (mPDeC2)");
   if (p->precision < 0 || p->precision > 2) return fail(SWM_ERR_PARAM, "unknown precision");
   if (p->solver != SWM_SOLVER_CSR && p->solver != SWM_SOLVER_STENCIL)
     return fail(SWM_ERR_PARAM, "unknown solver");
@@ -194,9 +200,175 @@ static void prof_mark(swm_solver* s, int cls) {
 }
 
 // Enqueue one complete mPDeC step on s->stream (dt read from s->dt_dev).
+// Patankar solves per step: mPDeC5 13, mPDeC2 2, mPEuler 1, explicit schemes none.
+static int solves_per_step(int timescheme) {
+  return timescheme == 5 ? 13 : (timescheme == 7 ? 2 : (timescheme == 6 ? 1 : 0));
+}
+
+// ---- explicit schemes (timediscretization.f90:104-451; build without PATANKAR) ----
+using Planes = std::array<double*, 3>;
+
+static Planes state_planes(swm_solver* s) { return {s->h, s->hu, s->hv}; }
+static Planes slot(swm_solver* s, int k) { return {s->ex[k][0], s->ex[k][1], s->ex[k][2]}; }
+
+// RHS of state X into R (all three components), mass fluxes to the slot-0 scratch.
+static int explicit_rhs(swm_solver* s, const Planes& X, const Planes& R) {
+  RhsArgs a = make_rhs_args(s, X[0], X[1], X[2], 0);
+  a.ut_h = R[0];
+  a.ut_hu = R[1];
+  a.ut_hv = R[2];
+  prof_mark(s, 0);
+  CK(launch_rhs(s, a));
+  prof_mark(s, -1);
+  return SWM_OK;
+}
+
+static int combo(swm_solver* s, int form, std::initializer_list<std::pair<double, Planes>> xs,
+                 std::initializer_list<std::pair<double, Planes>> ys, const Planes& out) {
+  ComboArgs c{};
+  c.n = (int)s->N;
+  c.form = form;
+  c.dt = s->dt_dev;
+  for (const auto& x : xs) {
+    c.c[c.nx] = x.first;
+    for (int v = 0; v < 3; ++v) c.X[c.nx][v] = x.second[v];
+    ++c.nx;
+  }
+  for (const auto& y : ys) {
+    c.d[c.ny] = y.first;
+    for (int v = 0; v < 3; ++v) c.Y[c.ny][v] = y.second[v];
+    ++c.ny;
+  }
+  for (int v = 0; v < 3; ++v) c.out[v] = out[v];
+  CK(launch_combo(c, s->stream));
+  return SWM_OK;
+}
+
+#define XCK(x)                 \
+  do {                         \
+    int rc_ = (x);             \
+    if (rc_) return rc_;       \
+  } while (0)
+
+static int enqueue_explicit(swm_solver* s) {
+  const Planes U = state_planes(s);
+  switch (s->p.timescheme) {
+    case 1: {  // forward Euler: U = K0 + Ut dt
+      const Planes R = slot(s, 0);
+      XCK(explicit_rhs(s, U, R));
+      XCK(combo(s, kComboSsp, {{1.0, U}}, {{1.0, R}}, U));
+    } break;
+    case 2: {  // SSPRK(5,4) (timediscretization.f90:128-189)
+      const Planes K0 = slot(s, 0), K1 = slot(s, 1), K2 = slot(s, 2), K3 = slot(s, 3),
+                   K4 = slot(s, 4), R = slot(s, 5), R2 = slot(s, 6);
+      for (int v = 0; v < 3; ++v)
+        CK(cudaMemcpyAsync(K0[v], U[v], sizeof(double) * s->N, cudaMemcpyDeviceToDevice,
+                           s->stream));
+      XCK(explicit_rhs(s, K0, R));
+      XCK(combo(s, kComboSsp, {{1.00000000000000, K0}}, {{0.39175222700392, R}}, K1));
+      XCK(explicit_rhs(s, K1, R));
+      XCK(combo(s, kComboSsp, {{0.44437049406734, K0}, {0.55562950593266, K1}},
+                {{0.36841059262959, R}}, K2));
+      XCK(explicit_rhs(s, K2, R));
+      XCK(combo(s, kComboSsp, {{0.62010185138540, K0}, {0.37989814861460, K2}},
+                {{0.25189177424738, R}}, K3));
+      XCK(explicit_rhs(s, K3, R));
+      XCK(combo(s, kComboSsp, {{0.17807995410773, K0}, {0.82192004589227, K3}},
+                {{0.54497475021237, R}}, K4));
+      XCK(explicit_rhs(s, K4, R2));  // K5 = R (the fourth stage's Ut), R2 the fifth's
+      XCK(combo(s, kComboSsp,
+                {{0.00683325884039, K0}, {0.51723167208978, K2}, {0.12759831133288, K3},
+                 {0.34833675773694, K4}},
+                {{0.08460416338212, R}, {0.22600748319395, R2}}, U));
+    } break;
+    case 3: {  // RK65 (timediscretization.f90:247-348); UN0 is U until the final update
+      static const double A[6][5] = {{0., 0., 0., 0., 0.},
+                                     {0.25, 0., 0., 0., 0.},
+                                     {0.125, 0.125, 0., 0., 0.},
+                                     {0., 0., 0.5, 0., 0.},
+                                     {0.1875, -0.375, 0.375, 0.5625, 0.},
+                                     {-0.42857142857142855, 1.1428571428571428, 0.8571428571428571,
+                                      -1.7142857142857142, 1.1428571428571428}};
+      static const double b[6] = {0.077777777777777778, 0., 0.35555555555555556,
+                                  0.13333333333333333, 0.35555555555555556, 0.077777777777777778};
+      const Planes St = slot(s, 6);
+      XCK(explicit_rhs(s, U, slot(s, 0)));
+      for (int st = 1; st <= 5; ++st) {
+        ComboArgs c{};
+        c.n = (int)s->N;
+        c.form = kComboRk;
+        c.dt = s->dt_dev;
+        c.nx = 1;
+        for (int v = 0; v < 3; ++v) c.X[0][v] = U[v];
+        c.ny = st;
+        for (int j = 0; j < st; ++j) {
+          c.d[j] = A[st][j];
+          for (int v = 0; v < 3; ++v) c.Y[j][v] = s->ex[j][v];
+        }
+        for (int v = 0; v < 3; ++v) c.out[v] = St[v];
+        CK(launch_combo(c, s->stream));
+        XCK(explicit_rhs(s, St, slot(s, st)));
+      }
+      ComboArgs c{};
+      c.n = (int)s->N;
+      c.form = kComboRk;
+      c.dt = s->dt_dev;
+      c.nx = 1;
+      c.ny = 6;
+      for (int v = 0; v < 3; ++v) {
+        c.X[0][v] = U[v];
+        c.out[v] = U[v];
+      }
+      for (int j = 0; j < 6; ++j) {
+        c.d[j] = b[j];
+        for (int v = 0; v < 3; ++v) c.Y[j][v] = s->ex[j][v];
+      }
+      CK(launch_combo(c, s->stream));
+    } break;
+    case 4: {  // DeC5 (timediscretization.f90:353-451): Ua(1) = U, Ua(2..4), FUp(1..4)
+      const Planes Ua[5] = {Planes{}, U, slot(s, 0), slot(s, 1), slot(s, 2)};
+      Planes F[5] = {Planes{}, slot(s, 3), slot(s, 3), slot(s, 3), slot(s, 3)};
+      XCK(explicit_rhs(s, U, F[1]));  // FUp(1..4) = F(U^n), one copy
+      for (int kk = 1; kk <= 5; ++kk) {
+        const int mlo = (kk == 5) ? 4 : 2;
+        for (int ii = mlo; ii <= 4; ++ii) {
+          ComboArgs c{};
+          c.n = (int)s->N;
+          c.form = kComboDec;
+          c.dt = s->dt_dev;
+          c.nx = 1;
+          c.ny = 4;
+          for (int v = 0; v < 3; ++v) {
+            c.X[0][v] = U[v];  // Ua(1)
+            c.out[v] = (kk == 5) ? U[v] : Ua[ii][v];  // the last correction is the new U
+          }
+          for (int jj = 1; jj <= 4; ++jj) {
+            c.d[jj - 1] = kTheta5[ii - 1][jj - 1];
+            for (int v = 0; v < 3; ++v) c.Y[jj - 1][v] = F[jj][v];
+          }
+          CK(launch_combo(c, s->stream));
+        }
+        if (kk != 5)
+          for (int ii = 2; ii <= 4; ++ii) {
+            F[ii] = slot(s, 2 + ii);  // FUp(2..4) in slots 4..6
+            XCK(explicit_rhs(s, Ua[ii], F[ii]));
+          }
+      }
+    } break;
+    default:
+      return fail(SWM_ERR_PARAM, "not an explicit scheme");
+  }
+  return SWM_OK;
+}
+
 static int enqueue_step(swm_solver* s) {
-  const bool two = (s->p.timescheme == 7);
-  const int ms = two ? 2 : 4, kc = two ? 2 : 5;
+  if (s->p.timescheme <= 4) {
+    CK(cudaMemsetAsync(&s->ctl->iters[0], 0, sizeof(int) * (kMaxSolves + 1), s->stream));
+    s->n_solves = 0;
+    return enqueue_explicit(s);
+  }
+  const bool two = (s->p.timescheme != 5);  // mPDeC2 or mPEuler: MSteps = 2
+  const int ms = two ? 2 : 4, kc = two ? (s->p.timescheme == 7 ? 2 : 1) : 5;
   const bool csr = (s->p.solver == SWM_SOLVER_CSR);
   const bool compat = two && s->p.mpdec2_compat;
   CK(cudaMemsetAsync(&s->ctl->iters[0], 0, sizeof(int) * (kMaxSolves + 1), s->stream));
@@ -418,7 +590,10 @@ int swm_create(const swm_params* p, swm_handle* out) {
   }
   AL(s->xa, N);
   AL(s->xb, N);
-  if (p->timescheme == 7 && p->mpdec2_compat) AL(s->rhs_compat, N);
+  if ((p->timescheme == 7 || p->timescheme == 6) && p->mpdec2_compat) AL(s->rhs_compat, N);
+  if (p->timescheme <= 4)
+    for (int k = 0; k < 7; ++k)
+      for (int v = 0; v < 3; ++v) AL(s->ex[k][v], N);
   if (p->well_balanced) {
     AL(s->fxwb, 3 * nfx);
     AL(s->fywb, 3 * nfy);
@@ -704,7 +879,7 @@ int swm_step(swm_handle s, double t, double dt) {
   CK(cudaMemcpyAsync(s->h_ctl, s->ctl, sizeof(JacobiCtl), cudaMemcpyDeviceToHost, s->stream));
   CK(cudaStreamSynchronize(s->stream));
   if (s->n_solves == 0) {  // graph built without a host pass: count solves
-    s->n_solves = (s->p.timescheme == 7) ? 2 : 13;
+    s->n_solves = solves_per_step(s->p.timescheme);
   }
   const JacobiCtl& c = *s->h_ctl;
   swm_stats& st = s->stats;
@@ -853,17 +1028,20 @@ int swm_debug_rhs(swm_handle s, const double* U, double* Ut, double* FX, double*
   double *h = s->hbuf[1][0], *hu = s->hum[1], *hv = s->hvm[1];
   int rc = upload_ghosted(s, U, h, hu, hv);
   if (rc) return rc;
-  double *dfx = nullptr, *dfy = nullptr, *ds = nullptr;
+  double *dfx = nullptr, *dfy = nullptr, *ds = nullptr, *dh = nullptr;
   CK(cudaMalloc(&dfx, 3 * nfx * sizeof(double)));
   CK(cudaMalloc(&dfy, 3 * nfy * sizeof(double)));
   CK(cudaMalloc(&ds, 3 * N * sizeof(double)));
+  CK(cudaMalloc(&dh, N * sizeof(double)));
   RhsArgs a = make_rhs_args(s, h, hu, hv, 1);
   a.fx_full = dfx;
   a.fy_full = dfy;
   a.s_full = ds;
+  a.ut_h = dh;  // Ut(1), as the build without PATANKAR computes it
   cudaError_t e = launch_rhs(s, a);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);  // s->stream is non-blocking
-  std::vector<double> hfx(3 * nfx), hfy(3 * nfy), hs(3 * N), hut(N), hvt(N);
+  std::vector<double> hfx(3 * nfx), hfy(3 * nfy), hs(3 * N), hht(N), hut(N), hvt(N);
+  if (e == cudaSuccess) e = cudaMemcpy(hht.data(), dh, N * sizeof(double), cudaMemcpyDeviceToHost);
   if (e == cudaSuccess) e = cudaMemcpy(hfx.data(), dfx, 3 * nfx * sizeof(double), cudaMemcpyDeviceToHost);
   if (e == cudaSuccess) e = cudaMemcpy(hfy.data(), dfy, 3 * nfy * sizeof(double), cudaMemcpyDeviceToHost);
   if (e == cudaSuccess) e = cudaMemcpy(hs.data(), ds, 3 * N * sizeof(double), cudaMemcpyDeviceToHost);
@@ -872,13 +1050,14 @@ int swm_debug_rhs(swm_handle s, const double* U, double* Ut, double* FX, double*
   cudaFree(dfx);
   cudaFree(dfy);
   cudaFree(ds);
+  cudaFree(dh);
   if (e != cudaSuccess) return fail(SWM_ERR_CUDA, cudaGetErrorString(e));
   // to the reference's column-major (3, ., .) layouts
   for (size_t j = 0; j < ny; ++j)
     for (size_t i = 0; i < nx; ++i) {
       size_t c = j * nx + i;
       if (Ut) {
-        Ut[3 * c] = 0.0;
+        Ut[3 * c] = hht[c];
         Ut[3 * c + 1] = hut[c];
         Ut[3 * c + 2] = hvt[c];
       }

@@ -380,6 +380,39 @@ cudaError_t launch_assemble(const AssembleArgs& a, bool csr, cudaStream_t s) {
 }
 
 // ---------------------------------------------------------------------------
+// Explicit schemes (timediscretization.f90:104-451): stage combinations.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) combo_kernel(const ComboArgs a) {
+  const double dt = *a.dt;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < a.n; k += gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int v = 0; v < 3; ++v) {
+      double acc;
+      if (a.form == kComboSsp) {
+        acc = a.c[0] * a.X[0][v][k];
+        for (int i = 1; i < a.nx; ++i) acc = acc + a.c[i] * a.X[i][v][k];
+        for (int j = 0; j < a.ny; ++j) acc = acc + a.d[j] * a.Y[j][v][k] * dt;
+      } else if (a.form == kComboRk) {
+        double sum = a.d[0] * a.Y[0][v][k];
+        for (int j = 1; j < a.ny; ++j) sum = sum + a.d[j] * a.Y[j][v][k];
+        acc = a.X[0][v][k] + sum * dt;
+      } else {
+        acc = a.X[0][v][k];
+        for (int j = 0; j < a.ny; ++j) acc = acc + dt * a.d[j] * a.Y[j][v][k];
+      }
+      a.out[v][k] = acc;
+    }
+  }
+}
+
+cudaError_t launch_combo(const ComboArgs& a, cudaStream_t s) {
+  int blocks = (a.n + 255) / 256;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  combo_kernel<<<blocks, 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
 // Jacobi (jacobi_iteration.f90:52-87): x^{k+1} = (b - L x^k)/D from x^0 = b,
 // residual mean|x^{k+1}-x^k|, stop when <= tol or at maxIter.
 // One cooperative persistent launch per solve; passes separated by a bounded

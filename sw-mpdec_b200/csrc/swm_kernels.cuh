@@ -157,6 +157,25 @@ cudaError_t launch_planes_to_ghosted(const double* h, const double* hu, const do
                                      int ny, double* G, double* Vg, cudaStream_t s);
 cudaError_t launch_summary(const double* h, int n, double* out /*[2]*/, cudaStream_t s);
 
+// Stage combinations of the explicit schemes, out[v] for v = h, hu, hv (FP64, each
+// product and sum rounded in the reference's order; out may alias X[0]):
+//  kComboSsp  sum_i c_i X_i + sum_j (d_j Y_j) dt      SSPRK(5,4), forward Euler
+//  kComboRk   X_0 + (sum_j d_j Y_j) dt                RK65
+//  kComboDec  X_0 + sum_j (dt d_j) Y_j                DeC5
+enum { kComboSsp = 0, kComboRk = 1, kComboDec = 2 };
+constexpr int kComboMax = 6;
+struct ComboArgs {
+  int n;        // cells
+  int form;
+  int nx, ny;   // terms in X and Y
+  double c[kComboMax], d[kComboMax];
+  const double* dt;  // device scalar
+  const double* X[kComboMax][3];
+  const double* Y[kComboMax][3];
+  double* out[3];
+};
+cudaError_t launch_combo(const ComboArgs& a, cudaStream_t s);
+
 // Initial conditions and the L1 error on the device (swm_ic.cu).
 struct IcArgs {
   Grid gr;

@@ -31,6 +31,7 @@ struct RhsArgs {
   const double* hv;     // state planes [ny][nx]
   double* ut_hu;
   double* ut_hv;        // momentum RHS [ny][nx]
+  double* ut_h;         // nullable: mass RHS Ut(1) (build without PATANKAR, explicit schemes)
   double* fxm;          // mass flux at x faces [ny][nx+1] (face f = left face of cell f)
   double* fym;          // mass flux at y faces [ny+1][nx]
   double* fx_full;      // nullable: [3][ny][nx+1]
@@ -535,6 +536,13 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const i
     } else {
       a.ut_hu[kc] = s[1] - (fxr[1] - fxl[1]) * gr.rdx - (fyt[1] - fyb[1]) * gr.rdy;
       a.ut_hv[kc] = s[2] - (fxr[2] - fxl[2]) * gr.rdx - (fyt[2] - fyb[2]) * gr.rdy;
+    }
+    if (a.ut_h) {  // Ut(1) = S(1) - dFX(1)/dx - dFY(1)/dy (finitevolume.f90:530-533)
+      if constexpr (EX)
+        a.ut_h[kc] = s[0] - div_rn(fxr[0] - fxl[0], gr.dx, gr.rdx) -
+                     div_rn(fyt[0] - fyb[0], gr.dy, gr.rdy);
+      else
+        a.ut_h[kc] = s[0] - (fxr[0] - fxl[0]) * gr.rdx - (fyt[0] - fyb[0]) * gr.rdy;
     }
     a.fxm[kx] = fxl[0];
     a.fym[ky] = fyb[0];

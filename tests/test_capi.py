@@ -66,7 +66,7 @@ def test_params_default_and_validation_without_gpu():
     h = ctypes.c_void_p()
     bad = swm.make_params(2, 32, (0.0, 0.0), (2.0, 1.0))
     assert lib.swm_create(ctypes.byref(bad), ctypes.byref(h)) == -1
-    bad = swm.make_params(64, 32, (0.0, 0.0), (2.0, 1.0), timescheme=4)
+    bad = swm.make_params(64, 32, (0.0, 0.0), (2.0, 1.0), timescheme=8)
     assert lib.swm_create(ctypes.byref(bad), ctypes.byref(h)) == -1
     assert b"timescheme" in lib.swm_last_error()
     bad = swm.make_params(64, 32, (0.0, 0.0), (2.0, 1.0), jacobi_block=9)

@@ -226,3 +226,46 @@ def test_l1_error_postprocessing():
     assert np.all(r.l1_error(1, t=0.0) == 0.0)
     assert r.l1_error(1, t=0.5)[0] > 1e-3
     assert np.allclose(r.l1_error(1, t=4.0 / 2.0 * 2), 0.0, atol=1e-12)  # period 4 in x and y
+
+
+def test_explicit_schemes_oracle():
+    # forward Euler is U + dt Ut with Ut(1) from the mass fluxes (build without
+    # PATANKAR); every explicit scheme conserves mass exactly on a periodic grid and
+    # the high-order ones agree with each other far better than with Euler
+    c = cases.case("vortex", n=24)
+    P0 = cases.cell_averages(c)
+    res = {}
+    for ts in (1, 2, 3, 4):
+        o = O.Oracle(O.make_params(c["nx"], c["ny"], c["x0"], c["x1"], g=c["g"], cfl=c["cfl"],
+                                   timescheme=ts))
+        o.set_planes(P0)
+        if ts == 1:
+            Ut = o.rhs()["Ut"]                     # (ny, nx, 3) interior RHS
+            o.set_planes(P0)
+        dt = 0.25 * o.timestep()
+        o.step(0.0, dt)
+        P = o.get_planes()
+        if ts == 1:
+            assert np.array_equal(P, P0 + np.moveaxis(Ut, -1, 0) * dt)
+        assert abs(P[0].sum() - P0[0].sum()) <= 1e-12 * P0[0].sum()
+        res[ts] = P
+    d_hi = max(np.abs(res[a] - res[b]).max() for a, b in ((2, 3), (3, 4), (2, 4)))
+    d_lo = np.abs(res[1] - res[3]).max()
+    assert d_hi < 1e-2 * d_lo, (d_hi, d_lo)
+
+
+def test_mpeuler_is_one_mpdec2_correction():
+    # mPEuler (KCorr 1) and mPDeC2 (KCorr 2): both keep h >= 0 on a dry dam break and
+    # differ by mPDeC2's second correction
+    c = cases.case("dambreak", n=24)
+    P0 = cases.cell_averages(c)
+    out = {}
+    for ts in (6, 7):
+        o = O.Oracle(O.make_params(c["nx"], c["ny"], c["x0"], c["x1"], g=c["g"], cfl=c["cfl"],
+                                   timescheme=ts))
+        o.set_planes(P0)
+        o.step(0.0, o.timestep())
+        out[ts] = o.get_planes()
+        assert out[ts][0].min() >= 0.0
+    assert not np.array_equal(out[6], out[7])
+    assert abs(out[6][0].sum() - out[7][0].sum()) <= 1e-12 * out[7][0].sum()  # mass
