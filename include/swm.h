@@ -144,6 +144,21 @@ SWM_API int swm_init_wb_ic(swm_handle h, int ic, const double *par, int npar);
 SWM_API int swm_l1_error(swm_handle h, int ic, const double *par, int npar, double t,
                          double l1[3]);
 
+/* WriteSolutionToDisk(t) (output.f90:29-185), formatted on the device: SOLUTION_* and
+ * ERROR_* files in `directory` named as TIMESTAMP does, Tecplot (which_output 2),
+ * Octave (1) or both (3), every value as (SP,ES21.14E2) with |v| < 1e-70 printed as 0.
+ * SOLUTION holds the barycentres, V = ConsToPrim(U) and the cell-averaged bathymetry;
+ * ERROR holds U - Uexact(ic, t) (par/npar as for swm_fill_ic).  flags
+ * SWM_OUT_V_LAST_RHS writes, for mPDeC5, the V the reference's BoundaryConditions left
+ * behind: that of the last RHS input of the step (Ua(4) of correction 4). */
+#define SWM_OUT_V_LAST_RHS 1
+SWM_API int swm_write_output(swm_handle h, double t, int which_output, int ic, const double *par,
+                             int npar, const char *directory, int flags);
+/* WriteMeshToDisk (output.f90:190-231): MESH_CoordinateX.dat, MESH_CoordinateY.dat. */
+SWM_API int swm_write_mesh(swm_handle h, const char *directory);
+/* n values as 21-character (SP,ES21.14E2) fields, back to back in out[21*n] (no NUL). */
+SWM_API int swm_debug_format(swm_handle h, const double *x, int n, char *out);
+
 /* TimeStep() (equation.f90:791-837): CFL time step of the current state. */
 SWM_API int swm_timestep(swm_handle h, double *dt_min);
 

@@ -240,6 +240,13 @@ def quadrature():
     return n, w
 
 
+def bathymetry(params, x, y):
+    """Bathymetry b(x, y) of the params (equation.f90:419-450), host libm."""
+    b = np.zeros(1)
+    _lib().orc_bathymetry(ctypes.byref(params), float(x), float(y), _dp(b), None, None)
+    return float(b[0])
+
+
 def theta_mpdec5():
     lib = _lib()
     th, beta = np.zeros(16), np.zeros(4)

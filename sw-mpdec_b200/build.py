@@ -8,6 +8,7 @@ Translation units and their floating-point flags:
   swm_batch.cu      batched ensembles
   swm_noalloc.cu    allocation-free Jacobi entry point
   swm_ic.cu         -fmad=false  (initial conditions, L1 error)
+  swm_output.cu     -fmad=false  (formatted solution files)
 Usage: python sw-mpdec_b200/build.py [--verbose] [--force]
 """
 import os
@@ -30,6 +31,7 @@ UNITS = [
     ("swm_batch.cu", []),
     ("swm_noalloc.cu", []),
     ("swm_ic.cu", ["-fmad=false"]),
+    ("swm_output.cu", ["-fmad=false"]),
 ]
 
 

@@ -92,6 +92,13 @@ struct swm_solver {
   double* summary = nullptr;
   double* l1_scratch = nullptr;  // L1 error: 3 * kIcMaxBlocks partials + 3 results
   double* ex[7][3] = {};          // explicit schemes: 7 stage slots of (h, hu, hv) planes
+  // formatted output: value planes (V, Bath, Error) and line buffers
+  double* out_planes = nullptr;  // 5 planes: u, v, Bath, error h, error hu (+ error hv below)
+  double* out_err_hv = nullptr;
+  bool have_bath = false;
+  char* out_dev = nullptr;
+  char* out_host = nullptr;  // pinned
+  size_t out_cap = 0;
   double* stage = nullptr;  // ghosted staging (3*(nx+6)*(ny+6))
   double* stage2 = nullptr;
   // pinned host mirrors
@@ -684,6 +691,8 @@ int swm_destroy(swm_handle s) {
   if (s->h_ctl) cudaFreeHost(s->h_ctl);
   if (s->h_lam) cudaFreeHost(s->h_lam);
   if (s->h_bad) cudaFreeHost(s->h_bad);
+  if (s->out_dev) cudaFree(s->out_dev);
+  if (s->out_host) cudaFreeHost(s->out_host);
   if (s->stream) cudaStreamDestroy(s->stream);
   delete s;
   return SWM_OK;
@@ -806,6 +815,192 @@ int swm_l1_error(swm_handle s, int ic, const double* par, int npar, double t, do
   CK(launch_l1_error(a, s->l1_scratch, out, s->stream));
   CK(cudaMemcpyAsync(l1, out, 3 * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
   CK(cudaStreamSynchronize(s->stream));
+  return SWM_OK;
+}
+
+// ---- formatted output (output.f90) ----
+static int out_buffers(swm_solver* s, size_t bytes) {
+  if (bytes <= s->out_cap) return SWM_OK;
+  if (s->out_dev) cudaFree(s->out_dev);
+  if (s->out_host) cudaFreeHost(s->out_host);
+  s->out_dev = nullptr;
+  s->out_host = nullptr;
+  s->out_cap = 0;
+  if (cudaMalloc(&s->out_dev, bytes) != cudaSuccess ||
+      cudaMallocHost(&s->out_host, bytes) != cudaSuccess)
+    return fail(SWM_ERR_ALLOC, "output line buffers");
+  s->out_cap = bytes;
+  return SWM_OK;
+}
+
+// TIMESTAMP (output.f90:375-395): F15.7 of the time with blanks as zeros
+static std::string timestamp(const char* name, double t) {
+  char buf[64];
+  snprintf(buf, sizeof(buf), "%15.7f", t);
+  for (char* c = buf; *c; ++c)
+    if (*c == ' ') *c = '0';
+  return std::string(name) + "_" + buf;
+}
+
+static std::string trimmed(const char* fmt, double v) {
+  char buf[64];
+  snprintf(buf, sizeof(buf), fmt, v);
+  const char* p = buf;
+  while (*p == ' ') ++p;
+  return p;
+}
+
+// Formats the lines on the device, copies them back and writes header + lines.
+static int write_lines(swm_solver* s, const std::string& path, const std::string& header,
+                       OutLines ol) {
+  const size_t lw = out_line_width(ol), bytes = lw * s->N;
+  int rc = out_buffers(s, bytes);
+  if (rc) return rc;
+  ol.out = s->out_dev;
+  CK(launch_out_lines(ol, s->stream));
+  CK(cudaMemcpyAsync(s->out_host, s->out_dev, bytes, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  FILE* f = fopen(path.c_str(), "w");
+  if (!f) return fail(SWM_ERR_PARAM, ("cannot open " + path).c_str());
+  const bool ok = fwrite(header.data(), 1, header.size(), f) == header.size() &&
+                  fwrite(s->out_host, 1, bytes, f) == bytes;
+  if (fclose(f) != 0 || !ok) return fail(SWM_ERR_PARAM, ("cannot write " + path).c_str());
+  return SWM_OK;
+}
+
+static const char* const kVarNames[4] = {"Depth", "VelocityX", "VelocityY", "Bathymetry"};
+
+// WriteDataToDisk_TECPLOT (output.f90:236-305) header
+static std::string tecplot_header(const swm_solver* s, double t) {
+  std::string h = "VARIABLES=\"CoordinateX\",\"CoordinateY\"";
+  for (const char* v : kVarNames) h += std::string(",\"") + v + "\"";
+  h += "\nZONE T=\"FV2D\",STRANDID=1,SOLUTIONTIME=" + trimmed("%15.8f", t) +
+       ", DATAPACKING=POINT, ZONETYPE=ORDERED, I=" + std::to_string(s->nx) +
+       ", J=" + std::to_string(s->ny) + "\n";
+  return h;
+}
+
+// WriteDataToDisk_OCTAVE (output.f90:310-370) header: names left-justified in 23
+static std::string octave_header() {
+  std::string h;
+  for (const char* v : kVarNames) {
+    std::string f(v);
+    f.resize(23, ' ');
+    h += f;
+  }
+  return h + "\n";
+}
+
+int swm_write_output(swm_handle s, double t, int which_output, int ic, const double* par,
+                     int npar, const char* directory, int flags) {
+  if (!s || !directory) return fail(SWM_ERR_PARAM, "null argument");
+  if (which_output < 1 || which_output > 3) return fail(SWM_ERR_PARAM, "which_output must be 1..3");
+  if (!s->have_state) return fail(SWM_ERR_STATE, "no state set");
+  IcArgs ia;
+  int rc = make_ic_args(s, ic, par, npar, t, s->h, s->hu, s->hv, &ia);
+  if (rc) return rc;
+  CK(cudaSetDevice(s->device));
+  const size_t N = s->N;
+  if (!s->out_planes) {
+    if ((rc = s->dalloc(&s->out_planes, 5 * N))) return rc;
+    if ((rc = s->dalloc(&s->out_err_hv, N))) return rc;
+  }
+  double *pu = s->out_planes, *pv = pu + N, *pb = pv + N, *e0 = pb + N, *e1 = e0 + N;
+  if (!s->have_bath) {  // Bath: cell averages of the bathymetry (finitevolume.f90:323-325)
+    CK(launch_bath_average(ia, pb, s->stream));
+    s->have_bath = true;
+  }
+  // U_NVisu(1:3) = V: ConsToPrim of the state, or of the last RHS input of the step
+  // (the reference's V after BoundaryConditions; mPDeC5: Ua(4) of correction 4)
+  const double *vh = s->h, *vhu = s->hu, *vhv = s->hv;
+  if ((flags & SWM_OUT_V_LAST_RHS) && s->p.timescheme == 5 && s->stats.steps > 0) {
+    vh = s->hbuf[3][0];
+    vhu = s->hum[3];
+    vhv = s->hvm[3];
+  }
+  CK(launch_prim(vh, vhu, vhv, pu, pv, (int)N, s->stream));
+  double* const ep[3] = {e0, e1, s->out_err_hv};
+  CK(launch_error_planes(ia, ep, s->stream));
+  const std::string dir = std::string(directory) + "/";
+  OutLines ol{};
+  ol.nx = s->nx;
+  ol.ny = s->ny;
+  ol.sep = 2;
+  ol.zero_small = 1;
+  ol.x0 = s->gr.x0;
+  ol.y0 = s->gr.y0;
+  ol.dx = s->gr.dx;
+  ol.dy = s->gr.dy;
+  ol.nval = 4;
+  for (int pass = 0; pass < 2; ++pass) {  // SOLUTION, then ERROR (output.f90:86-184)
+    const char* kind = pass == 0 ? "SOLUTION" : "ERROR";
+    if (pass == 0) {
+      ol.val[0] = vh;
+      ol.val[1] = pu;
+      ol.val[2] = pv;
+      ol.val[3] = pb;
+    } else {
+      ol.val[0] = e0;
+      ol.val[1] = e1;
+      ol.val[2] = s->out_err_hv;
+      ol.val[3] = nullptr;  // Error(nVar+1) = 0
+    }
+    if (which_output == 2 || which_output == 3) {
+      ol.ncoord = 2;
+      rc = write_lines(s, dir + timestamp((std::string(kind) + "_TEC").c_str(), t) + ".dat",
+                       tecplot_header(s, t), ol);
+      if (rc) return rc;
+    }
+    if (which_output == 1 || which_output == 3) {
+      ol.ncoord = 0;
+      rc = write_lines(s, dir + timestamp((std::string(kind) + "_OCT").c_str(), t) + ".dat",
+                       octave_header(), ol);
+      if (rc) return rc;
+    }
+  }
+  return SWM_OK;
+}
+
+// WriteMeshToDisk (output.f90:190-231): barycentre coordinates, one (SP,ES21.14E2) a line
+int swm_write_mesh(swm_handle s, const char* directory) {
+  if (!s || !directory) return fail(SWM_ERR_PARAM, "null argument");
+  CK(cudaSetDevice(s->device));
+  const int n[2] = {s->nx, s->ny};
+  const double x0[2] = {s->gr.x0, s->gr.y0}, dx[2] = {s->gr.dx, s->gr.dy};
+  for (int d = 0; d < 2; ++d) {
+    std::vector<double> c(n[d]);
+    for (int i = 0; i < n[d]; ++i) c[i] = (x0[d] + ((double)i) * dx[d]) + 0.5 * dx[d];
+    std::vector<char> txt(21 * (size_t)n[d]);
+    int rc = swm_debug_format(s, c.data(), n[d], txt.data());
+    if (rc) return rc;
+    const std::string path = std::string(directory) + (d ? "/MESH_CoordinateY.dat" : "/MESH_CoordinateX.dat");
+    FILE* f = fopen(path.c_str(), "w");
+    if (!f) return fail(SWM_ERR_PARAM, ("cannot open " + path).c_str());
+    fputs(d ? "CoordinateY\n" : "CoordinateX\n", f);
+    for (int i = 0; i < n[d]; ++i) {
+      fwrite(&txt[21 * (size_t)i], 1, 21, f);
+      fputc('\n', f);
+    }
+    if (fclose(f) != 0) return fail(SWM_ERR_PARAM, ("cannot write " + path).c_str());
+  }
+  return SWM_OK;
+}
+
+int swm_debug_format(swm_handle s, const double* x, int n, char* out) {
+  if (!s || (n > 0 && (!x || !out)) || n < 0) return fail(SWM_ERR_PARAM, "bad argument");
+  if (n == 0) return SWM_OK;
+  CK(cudaSetDevice(s->device));
+  double* dx = nullptr;
+  char* dout = nullptr;
+  CK(cudaMalloc(&dx, sizeof(double) * n));
+  cudaError_t e = cudaMalloc(&dout, 21 * (size_t)n);
+  if (e == cudaSuccess) e = cudaMemcpy(dx, x, sizeof(double) * n, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = launch_format_values(dx, n, dout, s->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+  if (e == cudaSuccess) e = cudaMemcpy(out, dout, 21 * (size_t)n, cudaMemcpyDeviceToHost);
+  cudaFree(dx);
+  cudaFree(dout);
+  if (e != cudaSuccess) return fail(SWM_ERR_CUDA, cudaGetErrorString(e));
   return SWM_OK;
 }
 

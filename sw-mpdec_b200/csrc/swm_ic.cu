@@ -188,7 +188,46 @@ __global__ void l1_final_kernel(const double* partial, int nblk, double dx, doub
   }
 }
 
+__global__ void __launch_bounds__(kIcThreads) error_planes_kernel(const IcArgs a, double* e0,
+                                                                   double* e1, double* e2) {
+  const int n = a.gr.nx * a.gr.ny;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+    double ue[3];
+    cell_average(a, c % a.gr.nx, c / a.gr.nx, ue);
+    e0[c] = a.h[c] - ue[0];
+    e1[c] = a.hu[c] - ue[1];
+    e2[c] = a.hv[c] - ue[2];
+  }
+}
+
+__global__ void __launch_bounds__(kIcThreads) bath_average_kernel(const IcArgs a, double* b) {
+  const Grid& gr = a.gr;
+  const int n = gr.nx * gr.ny;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+    const int i = c % gr.nx, j = c / gr.nx;
+    double s = 0.;
+    for (int ia = 0; ia < 4; ++ia) {
+      const double x = (gr.x0 + ((double)i) * gr.dx + 0.5 * gr.dx) + gr.qn[ia] * gr.dx;
+      for (int jb = 0; jb < 4; ++jb) {
+        const double y = (gr.y0 + ((double)j) * gr.dy + 0.5 * gr.dy) + gr.qn[jb] * gr.dy;
+        s = s + gr.wgp[ia][jb] * bathy_b(gr, x, y);
+      }
+    }
+    b[c] = s;
+  }
+}
+
 }  // namespace
+
+cudaError_t launch_error_planes(const IcArgs& a, double* const e[3], cudaStream_t s) {
+  error_planes_kernel<<<ic_blocks(a.gr.nx * a.gr.ny), kIcThreads, 0, s>>>(a, e[0], e[1], e[2]);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_bath_average(const IcArgs& a, double* b, cudaStream_t s) {
+  bath_average_kernel<<<ic_blocks(a.gr.nx * a.gr.ny), kIcThreads, 0, s>>>(a, b);
+  return cudaGetLastError();
+}
 
 int ic_blocks(int ncells) {
   int b = (ncells + kIcThreads - 1) / kIcThreads;

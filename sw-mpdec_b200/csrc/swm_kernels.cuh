@@ -176,6 +176,24 @@ struct ComboArgs {
 };
 cudaError_t launch_combo(const ComboArgs& a, cudaStream_t s);
 
+// Formatted output (swm_output.cu): one fixed-width line per cell.
+struct OutLines {
+  int nx, ny;
+  int ncoord;      // 0 or 2: the barycentre coordinates first
+  int nval;        // values per line after the coordinates (<= 4)
+  int sep;         // spaces after every field (2X)
+  int zero_small;  // print |v| < 1e-70 as 0
+  double x0, y0, dx, dy;
+  const double* val[4];  // planes [ny][nx]; null prints 0
+  char* out;             // nx*ny lines of out_line_width() bytes
+};
+size_t out_line_width(const OutLines& a);
+cudaError_t launch_out_lines(const OutLines& a, cudaStream_t s);
+cudaError_t launch_prim(const double* h, const double* hu, const double* hv, double* u, double* v,
+                        int n, cudaStream_t s);
+// n values as 21-character (SP,ES21.14E2) fields, back to back
+cudaError_t launch_format_values(const double* x, int n, char* out, cudaStream_t s);
+
 // Initial conditions and the L1 error on the device (swm_ic.cu).
 struct IcArgs {
   Grid gr;
@@ -193,6 +211,10 @@ int ic_blocks(int ncells);
 cudaError_t launch_ic_fill(const IcArgs& a, cudaStream_t s);
 // partial: 3 * ic_blocks(nx*ny) doubles of scratch; out: 3 doubles (device)
 cudaError_t launch_l1_error(const IcArgs& a, double* partial, double* out, cudaStream_t s);
+// Error(1:3) = U - Uexact(ic, t) into e[3] planes (output.f90:76-85; U read from a.h/hu/hv)
+cudaError_t launch_error_planes(const IcArgs& a, double* const e[3], cudaStream_t s);
+// Bath = 4x4 Gauss average of Bathymetry (finitevolume.f90:323-325) into b[N]
+cudaError_t launch_bath_average(const IcArgs& a, double* b, cudaStream_t s);
 void residual_limbs_host(double v, unsigned long long out[3]);
 
 }  // namespace swm

@@ -28,7 +28,8 @@ EXPORTS = [
     "swm_get_stream", "swm_profile_step", "swm_debug_rhs", "swm_debug_jacobi", "swm_batch_create", "swm_batch_destroy",
     "swm_batch_set_planes", "swm_batch_get_planes", "swm_batch_step", "swm_batch_cells",
     "swm_jacobi_noalloc", "swm_batch_get_stats", "swm_batch_get_stream",
-    "swm_fill_ic", "swm_init_wb_ic", "swm_l1_error",
+    "swm_fill_ic", "swm_init_wb_ic", "swm_l1_error", "swm_write_output", "swm_write_mesh",
+    "swm_debug_format",
 ]
 
 
@@ -87,6 +88,10 @@ def load():
     lib.swm_fill_ic.argtypes = [vp, ctypes.c_int, dp, ctypes.c_int]
     lib.swm_init_wb_ic.argtypes = [vp, ctypes.c_int, dp, ctypes.c_int]
     lib.swm_l1_error.argtypes = [vp, ctypes.c_int, dp, ctypes.c_int, ctypes.c_double, dp]
+    lib.swm_write_output.argtypes = [vp, ctypes.c_double, ctypes.c_int, ctypes.c_int, dp,
+                                     ctypes.c_int, ctypes.c_char_p, ctypes.c_int]
+    lib.swm_write_mesh.argtypes = [vp, ctypes.c_char_p]
+    lib.swm_debug_format.argtypes = [vp, dp, ctypes.c_int, ctypes.c_char_p]
     lib.swm_timestep.argtypes = [vp, dp]
     lib.swm_step.argtypes = [vp, ctypes.c_double, ctypes.c_double]
     lib.swm_run.argtypes = [vp, ctypes.c_double, ctypes.c_int, P(ctypes.c_int), dp]
@@ -216,6 +221,23 @@ class Solver:
         out = np.zeros(3)
         _check(self.lib.swm_l1_error(self.h, int(ic), p, n, float(t), _dp(out)))
         return out
+
+    def write_output(self, t, directory, which_output=2, ic=1, par=(), v_last_rhs=False):
+        """WriteSolutionToDisk(t): SOLUTION_* / ERROR_* files in `directory`."""
+        p, n, keep = self._par(par)
+        _check(self.lib.swm_write_output(self.h, float(t), int(which_output), int(ic), p, n,
+                                         os.fsencode(directory), 1 if v_last_rhs else 0))
+
+    def write_mesh(self, directory):
+        _check(self.lib.swm_write_mesh(self.h, os.fsencode(directory)))
+
+    def format_values(self, x):
+        """(SP,ES21.14E2) strings of the values, formatted on the device."""
+        x = np.ascontiguousarray(np.asarray(x, dtype=np.float64).ravel())
+        buf = ctypes.create_string_buffer(21 * max(x.size, 1))
+        _check(self.lib.swm_debug_format(self.h, _dp(x), int(x.size), buf))
+        raw = buf.raw[:21 * x.size].decode()
+        return [raw[21 * k:21 * k + 21] for k in range(x.size)]
 
     def timestep(self):
         dt = ctypes.c_double()

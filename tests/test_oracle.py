@@ -269,3 +269,29 @@ def test_mpeuler_is_one_mpdec2_correction():
         assert out[ts][0].min() >= 0.0
     assert not np.array_equal(out[6], out[7])
     assert abs(out[6][0].sum() - out[7][0].sum()) <= 1e-12 * out[7][0].sum()  # mass
+
+
+def test_output_formatting_restatement():
+    # (SP,ES21.14E2) of output.f90: sign always, 15 correctly rounded digits (ties to
+    # even on the exact binary value), two exponent digits or a field of asterisks
+    import output as OUT
+    assert OUT.es21(1.0) == "+1.00000000000000E+00"
+    assert OUT.es21(-0.0) == "-0.00000000000000E+00"
+    assert OUT.es21(123.456) == "+1.23456000000000E+02"
+    assert OUT.es21(1.0 + 2.0**-15) == "+1.00003051757812E+00"       # exact tie: even
+    assert OUT.es21(1.0 + 3 * 2.0**-15) == "+1.00009155273438E+00"   # exact tie: up
+    assert OUT.es21(9.9999999999999995) == "+1.00000000000000E+01"
+    assert OUT.es21(1e-100) == "*" * 21 and OUT.es21(1e100) == "*" * 21
+    assert OUT.es21(float("nan")).strip() == "NaN"
+    assert OUT.timestamp("SOLUTION_TEC", 0.1) == "SOLUTION_TEC_0000000.1000000"
+    txt = OUT.tecplot_text(0.25, 2, 1, (0.0, 0.0), (2.0, 1.0),
+                           [np.ones((1, 2)), np.zeros((1, 2)), np.full((1, 2), 1e-80),
+                            np.full((1, 2), -0.5)])
+    lines = txt.splitlines()
+    assert lines[0] == 'VARIABLES="CoordinateX","CoordinateY","Depth","VelocityX","VelocityY","Bathymetry"'
+    assert lines[1] == ('ZONE T="FV2D",STRANDID=1,SOLUTIONTIME=0.25000000, DATAPACKING=POINT, '
+                        'ZONETYPE=ORDERED, I=2, J=1')
+    assert lines[2].split() == ["+5.00000000000000E-01", "+5.00000000000000E-01",
+                                "+1.00000000000000E+00", "+0.00000000000000E+00",
+                                "+0.00000000000000E+00", "-5.00000000000000E-01"]
+    assert len(lines[2]) == 6 * 23
