@@ -11,6 +11,9 @@
 !   PostProcessing:              CALL SWM_Pull()  (copies U and V back)
 ! and one at start-up (after FillInitialConditions, main.f90:25):
 !   CALL SWM_Init()              (parameters, state, well-balanced reference)
+! Optionally the driver's initial condition, output and post-processing also run
+! on the device: SWM_FillInitialConditions, SWM_WriteSolution(t), SWM_WriteMesh,
+! SWM_PostProcessing (see the subroutines below).
 ! No Fortran compiler exists in the image this was written in; the interface
 ! follows the header's types one to one (c_int, c_double, c_ptr by value).
 !===============================================================================!
@@ -88,11 +91,46 @@ INTERFACE
   TYPE(C_PTR) FUNCTION swm_last_error() BIND(C, NAME="swm_last_error")
     IMPORT :: C_PTR
   END FUNCTION
+  INTEGER(C_INT) FUNCTION swm_fill_ic(h, ic, par, npar) BIND(C, NAME="swm_fill_ic")
+    IMPORT :: C_INT, C_PTR, C_DOUBLE
+    TYPE(C_PTR), VALUE :: h
+    INTEGER(C_INT), VALUE :: ic, npar
+    REAL(C_DOUBLE), INTENT(IN) :: par(*)
+  END FUNCTION
+  INTEGER(C_INT) FUNCTION swm_init_wb_ic(h, ic, par, npar) BIND(C, NAME="swm_init_wb_ic")
+    IMPORT :: C_INT, C_PTR, C_DOUBLE
+    TYPE(C_PTR), VALUE :: h
+    INTEGER(C_INT), VALUE :: ic, npar
+    REAL(C_DOUBLE), INTENT(IN) :: par(*)
+  END FUNCTION
+  INTEGER(C_INT) FUNCTION swm_l1_error(h, ic, par, npar, t, l1) BIND(C, NAME="swm_l1_error")
+    IMPORT :: C_INT, C_PTR, C_DOUBLE
+    TYPE(C_PTR), VALUE :: h
+    INTEGER(C_INT), VALUE :: ic, npar
+    REAL(C_DOUBLE), INTENT(IN) :: par(*)
+    REAL(C_DOUBLE), VALUE :: t
+    REAL(C_DOUBLE), INTENT(OUT) :: l1(3)
+  END FUNCTION
+  INTEGER(C_INT) FUNCTION swm_write_output(h, t, which, ic, par, npar, dir, flags) &
+      BIND(C, NAME="swm_write_output")
+    IMPORT :: C_INT, C_PTR, C_DOUBLE, C_CHAR
+    TYPE(C_PTR), VALUE :: h
+    REAL(C_DOUBLE), VALUE :: t
+    INTEGER(C_INT), VALUE :: which, ic, npar, flags
+    REAL(C_DOUBLE), INTENT(IN) :: par(*)
+    CHARACTER(KIND=C_CHAR), INTENT(IN) :: dir(*)
+  END FUNCTION
+  INTEGER(C_INT) FUNCTION swm_write_mesh(h, dir) BIND(C, NAME="swm_write_mesh")
+    IMPORT :: C_INT, C_PTR, C_CHAR
+    TYPE(C_PTR), VALUE :: h
+    CHARACTER(KIND=C_CHAR), INTENT(IN) :: dir(*)
+  END FUNCTION
 END INTERFACE
 
 TYPE(C_PTR), SAVE :: handle = C_NULL_PTR
 
 PUBLIC :: SWM_Init, SWM_TimeStep, SWM_Step, SWM_Pull, SWM_Finalize
+PUBLIC :: SWM_FillInitialConditions, SWM_WriteSolution, SWM_WriteMesh, SWM_PostProcessing
 
 CONTAINS
 
@@ -155,6 +193,51 @@ SUBROUTINE SWM_Pull()
   USE MOD_FiniteVolume2D_vars, ONLY: U, V
   CALL SWM_Check(swm_get_state(handle, U, V), "swm_get_state")
 END SUBROUTINE SWM_Pull
+
+! Optional device-side replacements of the driver's initialisation and output
+! (reference cases 1..6 of ExactFunction; no parameters).
+! CALL FillInitialConditions() (main.f90:23) -> CALL SWM_FillInitialConditions()
+SUBROUTINE SWM_FillInitialConditions()
+  USE MOD_FiniteVolume2D_vars, ONLY: InitialCondition
+  REAL(C_DOUBLE) :: par(1)
+  par = 0.0_C_DOUBLE
+  CALL SWM_Check(swm_fill_ic(handle, INT(InitialCondition, C_INT), par, 0_C_INT), &
+                 "swm_fill_ic")
+END SUBROUTINE SWM_FillInitialConditions
+
+! CALL WriteSolutionToDisk(t) (timediscretization.f90:52,87) -> CALL SWM_WriteSolution(t)
+SUBROUTINE SWM_WriteSolution(t)
+  USE MOD_FiniteVolume2D_vars, ONLY: InitialCondition, WhichOutput
+  REAL, INTENT(IN) :: t
+  REAL(C_DOUBLE) :: par(1)
+  par = 0.0_C_DOUBLE
+  IF (WhichOutput < 1 .OR. WhichOutput > 3) RETURN
+  CALL SWM_Check(swm_write_output(handle, REAL(t, C_DOUBLE), INT(WhichOutput, C_INT), &
+                 INT(InitialCondition, C_INT), par, 0_C_INT, "."//C_NULL_CHAR, 0_C_INT), &
+                 "swm_write_output")
+END SUBROUTINE SWM_WriteSolution
+
+! CALL WriteMeshToDisk() (timediscretization.f90:50) -> CALL SWM_WriteMesh()
+SUBROUTINE SWM_WriteMesh()
+  CALL SWM_Check(swm_write_mesh(handle, "."//C_NULL_CHAR), "swm_write_mesh")
+END SUBROUTINE SWM_WriteMesh
+
+! CALL PostProcessing() (main.f90:28): the L1 error at tEnd, written as
+! ErrorL1_XXXX_XXXX.dat (postprocessing.f90:52-58)
+SUBROUTINE SWM_PostProcessing()
+  USE MOD_FiniteVolume2D_vars, ONLY: InitialCondition, tEnd, nElemsX, nElemsY
+  REAL(C_DOUBLE) :: par(1), l1(3)
+  CHARACTER(LEN=255) :: FNAME
+  par = 0.0_C_DOUBLE
+  CALL SWM_Check(swm_l1_error(handle, INT(InitialCondition, C_INT), par, 0_C_INT, &
+                 REAL(tEnd, C_DOUBLE), l1), "swm_l1_error")
+  FNAME = 'ErrorL1_XXXX_XXXX.dat'
+  WRITE(FNAME(9:12),FMT="(I4.4)") nElemsX
+  WRITE(FNAME(14:17),FMT="(I4.4)") nElemsY
+  OPEN(666,FILE=TRIM(FNAME))
+  WRITE(666,*) l1(1:3)
+  CLOSE(666)
+END SUBROUTINE SWM_PostProcessing
 
 SUBROUTINE SWM_Finalize()
   INTEGER(C_INT) :: rc
