@@ -42,9 +42,9 @@ PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
 # summary under profiles/ holds the command and the counters.  Scaled by cells for
 # other grid sizes (the traffic of these kernels grows with the cell count).
 NCU_TRAFFIC_2048 = {
-    "rhs": (None, "profiles/rhs_split_island2048.md"),
-    "patankar_assemble": (None, "profiles/assemble_split_island2048.md"),
-    "jacobi": (None, "profiles/jacobi_stencil4_split_island2048.md"),
+    "rhs": (101284864.0 + 92335104.0, "profiles/rhs_split_island2048.md"),
+    "patankar_assemble": (None, "profiles/assemble_split_island2048.md"),  # k = 1 launch only
+    "jacobi": (463751936.0 + 65933056.0, "profiles/jacobi_stencil4_split_island2048.md"),
 }
 
 # Algorithmic bytes per cell-step of the whole mPDeC5 step: every phase reads its
