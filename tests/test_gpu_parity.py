@@ -113,6 +113,31 @@ def test_jacobi_bitwise(gpu, solver, block):
     assert np.array_equal(got, ref)
 
 
+@pytest.mark.parametrize("n", [96, 100])
+@pytest.mark.parametrize("block", [1, 2, 4])
+def test_jacobi_bitwise_wide(gpu, n, block):
+    # grids wider than one haloed tile, with 16-byte pair loads (even nx); 100 is not a
+    # multiple of the 64-wide tiles, so edge tiles hang over the grid
+    c, o, s = make_pair(gpu, "vortex", n, solver="stencil", block=block)
+    mass, diag, rhs = random_patankar_system(n * n, 11)
+    ref, k_ref = o.jacobi(mass, diag, rhs)
+    got, k, rc = s.debug_jacobi(mass, diag, rhs)
+    assert k == k_ref
+    assert np.array_equal(got, ref)
+
+
+@pytest.mark.parametrize("name", ["vortex", "dambreak"])
+def test_steps_exact_bitwise_wide(gpu, name):
+    c, o, s = make_pair(gpu, name, 96, solver="stencil", block=4)
+    for _ in range(2):
+        dt = o.timestep()
+        assert s.timestep() == dt
+        o.step(0.0, dt)
+        s.step(0.0, dt)
+    assert np.array_equal(s.get_planes(), o.get_planes())
+    assert list(s.stats()["jacobi_iters"][:13]) == list(o.last_jacobi_iters()[:13])
+
+
 def test_jacobi_maxiter_warning(gpu):
     c, o, s = make_pair(gpu, "vortex", 40, maxiter=3, solver="stencil", block=2)
     mass, diag, rhs = random_patankar_system(40 * 40, 5)
