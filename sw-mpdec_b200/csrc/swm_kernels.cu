@@ -6,16 +6,24 @@
 #include <cooperative_groups.h>
 
 #include <cstdio>
+#include <cstring>
 
 #include "swm_kernels.cuh"
 
 namespace swm {
 
 // ---------------------------------------------------------------------------
-// Residual limbs: |dx| in units of 2^-100 as three 40-bit integers.
-// Scaling by powers of two and flooring are exact in FP64, so the split is exact
-// (apart from truncation below 2^-100) and the integer sum is order-independent.
+// Residual limbs: |dx| in units of 2^-100 as three 40-bit integers,
+// X = floor(v * 2^100) = l2 * 2^80 + l1 * 2^40 + l0 (exact apart from the
+// truncation below 2^-100), so the integer sum is order-independent.  X is taken
+// from the bits of v: v = m * 2^(e - 1075) with the 53-bit significand m, hence
+// X = m * 2^(e - 975) and each limb is m shifted by (e - 975 - 40k), masked --
+// integer shifts only, no floating-point-to-integer conversions.
 // ---------------------------------------------------------------------------
+__host__ __device__ __forceinline__ unsigned long long shift_u64(unsigned long long m, int d) {
+  return d >= 0 ? (d < 64 ? m << d : 0ull) : (d > -64 ? m >> -d : 0ull);
+}
+
 __host__ __device__ inline void residual_limbs(double v, unsigned long long& l2,
                                                unsigned long long& l1, unsigned long long& l0) {
   const unsigned long long m40 = (1ull << 40) - 1;
@@ -25,14 +33,19 @@ __host__ __device__ inline void residual_limbs(double v, unsigned long long& l2,
     l0 = m40;
     return;
   }
-  double x = v * 0x1p100;
-  double q2 = floor(x * 0x1p-80);
-  double r = x - q2 * 0x1p80;
-  double q1 = floor(r * 0x1p-40);
-  double r0 = r - q1 * 0x1p40;
-  l2 = (unsigned long long)q2;
-  l1 = (unsigned long long)q1;
-  l0 = (unsigned long long)floor(r0);
+#ifdef __CUDA_ARCH__
+  const unsigned long long bits = (unsigned long long)__double_as_longlong(v);
+#else
+  unsigned long long bits;
+  memcpy(&bits, &v, sizeof bits);
+#endif
+  // v >= 0: no sign bit; e = 0 (zero, subnormal) scales as e = 1 without the hidden bit
+  const int e = (int)(bits >> 52);
+  const unsigned long long m = (bits & ((1ull << 52) - 1)) | (e ? (1ull << 52) : 0ull);
+  const int s = (e ? e : 1) - 975;
+  l2 = shift_u64(m, s - 80);  // < 2^40 since v < 2^20
+  l1 = shift_u64(m, s - 40) & m40;
+  l0 = shift_u64(m, s) & m40;
 }
 
 void residual_limbs_host(double v, unsigned long long out[3]) {
@@ -470,17 +483,39 @@ __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::);
 }
 
-// Per-thread residual limbs for sweep 0 (initial residual) and sweeps 1..kMaxBlock.
+// Per-thread residual sums for sweep 0 (initial residual) and sweeps 1..kMaxBlock.
+// Each |dx| (capped at 2^20; NaN counts as 2^20) is rounded to a multiple of 2^-100
+// and split exactly into parts h2 + h1 + h0, multiples of 2^-20, 2^-60 and 2^-100
+// with |h1| <= 2^-21, |h0| <= 2^-61: x + C - C rounds x to a multiple of 2^k for
+// C = 1.5 * 2^(52+k) and |x| < 2^(51+k), and the remainders are exact.  Each part
+// has at most 40 significant bits in its unit, so up to 2^13 of them sum exactly in
+// one FP64 accumulator (callers flush before that); the sums are exact integers in
+// their units, hence independent of the order of summation.
 struct Acc {
-  unsigned long long v[kMaxBlock + 1][3];
+  double s2[kMaxBlock + 1], s1[kMaxBlock + 1], s0[kMaxBlock + 1];
 };
+constexpr int kAccFlushCells = 4096;  // values per thread between flushes, < 2^13
 
-__device__ __forceinline__ void acc_put(unsigned long long* a3, double v) {
-  unsigned long long l2, l1, l0;
-  residual_limbs(v, l2, l1, l0);
-  a3[0] += l2;
-  a3[1] += l1;
-  a3[2] += l0;
+__device__ __forceinline__ void acc_zero(Acc& acc) {
+#pragma unroll
+  for (int t = 0; t <= kMaxBlock; ++t) {
+    acc.s2[t] = 0.;
+    acc.s1[t] = 0.;
+    acc.s0[t] = 0.;
+  }
+}
+
+template <int T>
+__device__ __forceinline__ void acc_put(Acc& acc, double v) {
+  const double a = v < 1048576.0 ? v : 1048576.0;
+  const double C2 = 0x1.8p32, C1 = 0x1.8p-8, C0 = 0x1.8p-48;
+  const double h2 = __dsub_rn(__dadd_rn(a, C2), C2);
+  const double r = __dsub_rn(a, h2);
+  const double h1 = __dsub_rn(__dadd_rn(r, C1), C1);
+  const double h0 = __dsub_rn(__dadd_rn(__dsub_rn(r, h1), C0), C0);
+  acc.s2[T] = __dadd_rn(acc.s2[T], h2);
+  acc.s1[T] = __dadd_rn(acc.s1[T], h1);
+  acc.s0[T] = __dadd_rn(acc.s0[T], h0);
 }
 
 // periodic index for -n <= g < 2n
@@ -490,13 +525,111 @@ __device__ __forceinline__ int wrap_near(int g, int n) {
   return g;
 }
 
+// Sweep T (1..TB) of a pass over a tile in shared memory: the cells of rows
+// T..HY-1-T and columns T..HX-1-T, from xp into xn.  The work unit is a pair of
+// adjacent cells (lx even, lx + 1) of one row: 16-byte loads of the six
+// coefficient pairs and of the centre, south and north pairs of x, 8-byte loads of
+// the west and east neighbours.  For odd T the first and last pairs of a row reach
+// one column past the region; those cells are computed and stored too, but no later
+// sweep reads them (sweep T+1 reads columns T..HX-1-T only), and their neighbour
+// loads stay inside the tile arrays since rows 0 and HY-1 are never swept.
+// Residuals count the tile's own cells: (lx - TB, ly - TB) < (cx_lim, cy_lim).
+__device__ __forceinline__ double2 lds2(const double* p) {
+  return *reinterpret_cast<const double2*>(p);
+}
+
+template <int TB, int T, bool RECIP>
+__device__ __forceinline__ void tile_sweep(const double* sm, const double* xp, double* xn,
+                                           int cx_lim, int cy_lim, Acc& acc) {
+  using G = JTile<TB>;
+  constexpr int HX = G::HX, HN = G::HN;
+  constexpr int P0 = T / 2, NP = (HX - T - 1) / 2 - P0 + 1;  // pairs covering [T, HX-T)
+  constexpr int NU = NP * (G::HY - 2 * T), NQ = (NU + JNT - 1) / JNT;
+  static_assert(HX % 2 == 0 && HN % 2 == 0, "16-byte pairs");
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) {
+    const int u = threadIdx.x + q * JNT;
+    if (NU % JNT != 0 && u >= NU) break;
+    const int ly = T + u / NP, lx = 2 * (P0 + u % NP);
+    const int c = ly * HX + lx;
+    const double2 cS = lds2(sm + c), cW = lds2(sm + HN + c), cE = lds2(sm + 2 * HN + c),
+                  cN = lds2(sm + 3 * HN + c), cD = lds2(sm + 4 * HN + c),
+                  cB = lds2(sm + 5 * HN + c);
+    const double2 xs = lds2(xp + c - HX), xc = lds2(xp + c), xq = lds2(xp + c + HX);
+    const double xw = xp[c - 1], xe = xp[c + 2];
+    // product = (((S x_S + W x_W) + E x_E) + N x_N); the zero centre slot of the
+    // reference CSR row adds an exact zero and is skipped.
+    double p0 = __dmul_rn(cS.x, xs.x), p1 = __dmul_rn(cS.y, xs.y);
+    p0 = __dadd_rn(p0, __dmul_rn(cW.x, xw));
+    p1 = __dadd_rn(p1, __dmul_rn(cW.y, xc.x));
+    p0 = __dadd_rn(p0, __dmul_rn(cE.x, xc.y));
+    p1 = __dadd_rn(p1, __dmul_rn(cE.y, xe));
+    p0 = __dadd_rn(p0, __dmul_rn(cN.x, xq.x));
+    p1 = __dadd_rn(p1, __dmul_rn(cN.y, xq.y));
+    double2 v;
+    v.x = RECIP ? __dmul_rn(__dsub_rn(cB.x, p0), cD.x) : __ddiv_rn(__dsub_rn(cB.x, p0), cD.x);
+    v.y = RECIP ? __dmul_rn(__dsub_rn(cB.y, p1), cD.y) : __ddiv_rn(__dsub_rn(cB.y, p1), cD.y);
+    *reinterpret_cast<double2*>(xn + c) = v;
+    if ((unsigned)(ly - TB) < (unsigned)cy_lim) {
+      if ((unsigned)(lx - TB) < (unsigned)cx_lim) acc_put<T>(acc, fabs(__dsub_rn(v.x, xc.x)));
+      if ((unsigned)(lx + 1 - TB) < (unsigned)cx_lim) acc_put<T>(acc, fabs(__dsub_rn(v.y, xc.y)));
+    }
+  }
+}
+
+// Sweeps T..Tp of a pass, each followed by a block barrier; xp ends on the last iterate.
+template <int TB, int T, bool RECIP>
+__device__ __forceinline__ void tile_sweeps(const double* sm, double*& xp, double*& xn, int Tp,
+                                            int cx_lim, int cy_lim, Acc& acc) {
+  if constexpr (T <= TB) {
+    if (T <= Tp) {
+      tile_sweep<TB, T, RECIP>(sm, xp, xn, cx_lim, cy_lim, acc);
+      __syncthreads();
+      double* tmp = xp;
+      xp = xn;
+      xn = tmp;
+      tile_sweeps<TB, T + 1, RECIP>(sm, xp, xn, Tp, cx_lim, cy_lim, acc);
+    }
+  }
+}
+
+// Block reduction of the per-thread sums into s_acc (sweeps 0..TB) as 40-bit limbs
+// [2^80, 2^40, 1] of 2^-100 units.  The parts' sums are exact integers below 2^53
+// in their units; carries normalise the (possibly negative) lower parts, and a
+// thread's top limb is capped at 2^40 - 1 (its sum is then >= 2^20, far above any
+// stop threshold).
+template <int TB>
+__device__ __forceinline__ void acc_reduce(Acc& acc, unsigned long long (*s_acc)[3]) {
+  const long long m40 = (1ll << 40) - 1;
+#pragma unroll
+  for (int t = 0; t <= TB; ++t) {
+    const long long S2 = __double2ll_rn(__dmul_rn(acc.s2[t], 0x1p20));
+    const long long S1 = __double2ll_rn(__dmul_rn(acc.s1[t], 0x1p60));
+    const long long S0 = __double2ll_rn(__dmul_rn(acc.s0[t], 0x1p100));
+    const long long n1 = S1 + (S0 >> 40);  // arithmetic shifts: floor division
+    const long long n2 = S2 + (n1 >> 40);
+    const unsigned long long limb[3] = {(unsigned long long)(n2 < m40 ? n2 : m40),
+                                        (unsigned long long)(n1 & m40),
+                                        (unsigned long long)(S0 & m40)};
+    acc.s2[t] = 0.;
+    acc.s1[t] = 0.;
+    acc.s0[t] = 0.;
+#pragma unroll
+    for (int l = 0; l < 3; ++l) {
+      unsigned long long v = warp_sum_u64(limb[l]);
+      if ((threadIdx.x & 31) == 0 && v) atomicAdd(&s_acc[t][l], v);
+    }
+  }
+}
+
 // One stencil pass of Tp <= TB sweeps over every tile of this CTA.  A tile is a
 // JBX x JBY block of cells plus a TB-cell halo in shared memory; sweep t updates
 // the region shrunk by t, so after Tp sweeps the tile interior holds x^{k+Tp},
 // bit-identical to Tp global sweeps.  Warps own rows, lanes own columns.
 template <int TB, bool RECIP, bool ONE_TILE>
 __device__ void stencil_tiles(const JacobiArgs& a, const double* xin, double* xout, int Tp,
-                              bool first, Acc& acc, double* sm, int tile_first) {
+                              bool first, Acc& acc, double* sm, int tile_first,
+                              unsigned long long (*s_acc)[3]) {
   using G = JTile<TB>;
   constexpr int HX = G::HX, HY = G::HY, HN = G::HN, NW = JNT / 32;
   double* sS = sm;
@@ -516,8 +649,16 @@ __device__ void stencil_tiles(const JacobiArgs& a, const double* xin, double* xo
   // ONE_TILE: exactly tile `tile_first` (ensembles); else every CTA-strided tile
   const int t_end = ONE_TILE ? tile_first + 1 : tx * ty;
   const int t_step = ONE_TILE ? 1 : gridDim.x;
+  // values a thread adds per sweep and tile: two per pair unit of sweep 1
+  constexpr int kPerTile = 2 * ((((HX - 2) / 2 + 1) * (HY - 2) + JNT - 1) / JNT);
+  int since_flush = 0;
   for (int tile = tile_first; tile < t_end; tile += t_step) {
     const int i0 = (tile % tx) * JBX, j0 = (tile / tx) * JBY;
+    const int cx_lim = min(JBX, nx - i0), cy_lim = min(JBY, ny - j0);
+    if (!ONE_TILE && (since_flush += kPerTile) > kAccFlushCells) {
+      acc_reduce<TB>(acc, s_acc);  // keep the per-thread part sums exact
+      since_flush = kPerTile;
+    }
     if (pairs) {
       // even nx, no multiple wrap: 16-byte pairs (gi even) never straddle the seam
       for (int ly = warp; ly < HY; ly += NW) {
@@ -561,36 +702,11 @@ __device__ void stencil_tiles(const JacobiArgs& a, const double* xin, double* xo
     if (first) {  // initial residual mean|0 - b| (jacobi_iteration.f90:69)
       for (int ly = TB + warp; ly < TB + JBY; ly += NW)
         for (int lx = TB + lane; lx < TB + JBX; lx += 32)
-          if (i0 + lx - TB < nx && j0 + ly - TB < ny) acc_put(acc.v[0], fabs(0. - sB[ly * HX + lx]));
+          if (i0 + lx - TB < nx && j0 + ly - TB < ny) acc_put<0>(acc, fabs(0. - sB[ly * HX + lx]));
     }
     double* xp = x0;
     double* xn = x1;
-#pragma unroll
-    for (int t = 1; t <= TB; ++t) {
-      if (t <= Tp) {
-        for (int ly = t + warp; ly < HY - t; ly += NW) {
-          const bool row_in = ly >= TB && ly < TB + JBY && j0 + ly - TB < ny;
-          for (int lx = t + lane; lx < HX - t; lx += 32) {
-            const int c = ly * HX + lx;
-            // product = (((S x_S + W x_W) + E x_E) + N x_N); the zero centre slot of the
-            // reference CSR row adds an exact zero and is skipped.
-            double p = __dmul_rn(sS[c], xp[c - HX]);
-            p = __dadd_rn(p, __dmul_rn(sW[c], xp[c - 1]));
-            p = __dadd_rn(p, __dmul_rn(sE[c], xp[c + 1]));
-            p = __dadd_rn(p, __dmul_rn(sN[c], xp[c + HX]));
-            const double xv = RECIP ? __dmul_rn(__dsub_rn(sB[c], p), sD[c])
-                                    : __ddiv_rn(__dsub_rn(sB[c], p), sD[c]);
-            xn[c] = xv;
-            if (row_in && lx >= TB && lx < TB + JBX && i0 + lx - TB < nx)
-              acc_put(acc.v[t], fabs(__dsub_rn(xv, xp[c])));
-          }
-        }
-        __syncthreads();
-        double* tmp = xp;
-        xp = xn;
-        xn = tmp;
-      }
-    }
+    tile_sweeps<TB, 1, RECIP>(sm, xp, xn, Tp, cx_lim, cy_lim, acc);
     for (int ly = TB + warp; ly < TB + JBY; ly += NW) {
       const int gj = j0 + ly - TB;
       if (gj >= ny) continue;
@@ -605,30 +721,25 @@ __device__ void stencil_tiles(const JacobiArgs& a, const double* xin, double* xo
 
 // One CSR pass (one sweep): sparse_matmul (jacobi_iteration.f90:25-43) + update.
 __device__ void csr_pass(const JacobiArgs& a, const double* xin, double* xout, bool first,
-                         Acc& acc) {
+                         Acc& acc, unsigned long long (*s_acc)[3]) {
   const int n = a.nx * a.ny;
-  for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < n; row += gridDim.x * blockDim.x) {
-    double prod = 0.;
-    for (int sp = a.rowstart[row]; sp <= a.rowstart[row + 1] - 1; ++sp)
-      prod = __dadd_rn(prod, __dmul_rn(a.mass[sp - 1], __ldcg(&xin[a.cols[sp - 1] - 1])));
-    const double xv = __ddiv_rn(__dsub_rn(a.b[row], prod), a.diag[row]);
-    xout[row] = xv;
-    acc_put(acc.v[1], fabs(__dsub_rn(xv, __ldcg(&xin[row]))));
-    if (first) acc_put(acc.v[0], fabs(0. - a.b[row]));
-  }
-}
-
-// Block reduction of the per-thread limbs into s_acc (sweeps 0..TB).
-template <int TB>
-__device__ __forceinline__ void acc_reduce(Acc& acc, unsigned long long (*s_acc)[3]) {
-#pragma unroll
-  for (int t = 0; t <= TB; ++t)
-#pragma unroll
-    for (int l = 0; l < 3; ++l) {
-      unsigned long long v = warp_sum_u64(acc.v[t][l]);
-      acc.v[t][l] = 0ull;
-      if ((threadIdx.x & 31) == 0 && v) atomicAdd(&s_acc[t][l], v);
+  const int stride = gridDim.x * blockDim.x;
+  // rows per thread between flushes of the part sums (every thread of the block
+  // takes part in a flush, so the count is the block's, not the thread's)
+  const long long rows_per_flush = (long long)kAccFlushCells * stride;
+  for (long long base = blockIdx.x * blockDim.x; base < n; base += rows_per_flush) {
+    if (base != blockIdx.x * blockDim.x) acc_reduce<1>(acc, s_acc);
+    const int end = (int)((n - base > rows_per_flush) ? base + rows_per_flush : n);
+    for (int row = (int)base + threadIdx.x; row < end; row += stride) {
+      double prod = 0.;
+      for (int sp = a.rowstart[row]; sp <= a.rowstart[row + 1] - 1; ++sp)
+        prod = __dadd_rn(prod, __dmul_rn(a.mass[sp - 1], __ldcg(&xin[a.cols[sp - 1] - 1])));
+      const double xv = __ddiv_rn(__dsub_rn(a.b[row], prod), a.diag[row]);
+      xout[row] = xv;
+      acc_put<1>(acc, fabs(__dsub_rn(xv, __ldcg(&xin[row]))));
+      if (first) acc_put<0>(acc, fabs(0. - a.b[row]));
     }
+  }
 }
 
 template <int TB, bool CSR, bool RECIP>
@@ -646,10 +757,7 @@ __global__ void __launch_bounds__(JNT, 2) jacobi_kernel(const JacobiArgs a) {
   int k = 0, final_k = 0;
   const int blk = CSR ? 1 : (a.block < 1 ? 1 : (a.block > TB ? TB : a.block));
   Acc acc;
-#pragma unroll
-  for (int t = 0; t <= kMaxBlock; ++t)
-#pragma unroll
-    for (int l = 0; l < 3; ++l) acc.v[t][l] = 0ull;
+  acc_zero(acc);
   for (;;) {
     int Tp = blk;
     if (a.maxiter - k < Tp) Tp = a.maxiter - k;
@@ -657,9 +765,9 @@ __global__ void __launch_bounds__(JNT, 2) jacobi_kernel(const JacobiArgs a) {
     for (int q = threadIdx.x; q < (kMaxBlock + 1) * 3; q += blockDim.x) (&s_acc[0][0])[q] = 0ull;
     __syncthreads();
     if (CSR)
-      csr_pass(a, xin, xout, first, acc);
+      csr_pass(a, xin, xout, first, acc, s_acc);
     else
-      stencil_tiles<TB, RECIP, false>(a, xin, xout, Tp, first, acc, jsm, blockIdx.x);
+      stencil_tiles<TB, RECIP, false>(a, xin, xout, Tp, first, acc, jsm, blockIdx.x, s_acc);
     acc_reduce<TB>(acc, s_acc);
     __syncthreads();
     const int slot = p % kResSlots;
@@ -703,7 +811,7 @@ __global__ void __launch_bounds__(JNT, 2) jacobi_kernel(const JacobiArgs a) {
         for (int q = threadIdx.x; q < (kMaxBlock + 1) * 3; q += blockDim.x)
           (&s_acc[0][0])[q] = 0ull;
         __syncthreads();
-        stencil_tiles<TB, RECIP, false>(a, xin, xout, stop, false, acc, jsm, blockIdx.x);
+        stencil_tiles<TB, RECIP, false>(a, xin, xout, stop, false, acc, jsm, blockIdx.x, s_acc);
         acc_reduce<TB>(acc, s_acc);
         if (!grid_barrier(ctl, a.spin_limit, &s_ok)) return;
         if (blockIdx.x == 0) {
@@ -913,10 +1021,7 @@ __global__ void __launch_bounds__(JNT, 2) jacobi_batch_kernel(const JacobiBatchA
   }
   if (!grid_barrier(a.ctl, a.spin_limit, &s_ok)) return;
   Acc acc;
-#pragma unroll
-  for (int t = 0; t <= kMaxBlock; ++t)
-#pragma unroll
-    for (int l = 0; l < 3; ++l) acc.v[t][l] = 0ull;
+  acc_zero(acc);
   int loaded = -1;
   for (;;) {
     for (int w = blockIdx.x; w < a.ntiles; w += gridDim.x) {
@@ -940,7 +1045,7 @@ __global__ void __launch_bounds__(JNT, 2) jacobi_batch_kernel(const JacobiBatchA
       if (s_active) {
         const double* xin = s_cur == 0 ? sd.b : (s_cur == 1 ? sd.xa : sd.xb);
         double* xout = s_cur == 1 ? sd.xb : sd.xa;
-        stencil_tiles<TB, RECIP, true>(sd, xin, xout, s_Tp, s_first != 0, acc, jsm, t.y);
+        stencil_tiles<TB, RECIP, true>(sd, xin, xout, s_Tp, s_first != 0, acc, jsm, t.y, s_acc);
         acc_reduce<TB>(acc, s_acc);
         __syncthreads();
         if (threadIdx.x < (TB + 1) * 3) {
