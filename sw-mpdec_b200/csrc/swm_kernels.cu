@@ -518,6 +518,15 @@ __device__ __forceinline__ void acc_put(Acc& acc, double v) {
   acc.s0[T] = __dadd_rn(acc.s0[T], h0);
 }
 
+// Every array a stencil pass copies with 16-byte cp.async starts on a 16-byte boundary.
+__host__ __device__ __forceinline__ bool arrays_aligned16(const JacobiArgs& a, const double* xin) {
+  const unsigned long long u = (unsigned long long)a.cS | (unsigned long long)a.cW |
+                               (unsigned long long)a.cE | (unsigned long long)a.cN |
+                               (unsigned long long)a.cD | (unsigned long long)a.b |
+                               (unsigned long long)xin;
+  return (u & 15ull) == 0;
+}
+
 // periodic index for -n <= g < 2n
 __device__ __forceinline__ int wrap_near(int g, int n) {
   if (g < 0) g += n;
@@ -643,8 +652,9 @@ __device__ void stencil_tiles(const JacobiArgs& a, const double* xin, double* xo
   const int nx = a.nx, ny = a.ny;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const bool small = (nx < HX) || (ny < HY);
-  // 16-byte pairs need an even first column (i0 - TB) and an even row pitch
-  const bool pairs = (TB % 2 == 0) && !small && (nx % 2 == 0);
+  // 16-byte pairs need an even first column (i0 - TB), an even row pitch and 16-byte
+  // aligned arrays (the allocation-free entry takes the caller's pointers as given)
+  const bool pairs = (TB % 2 == 0) && !small && (nx % 2 == 0) && arrays_aligned16(a, xin);
   const int tx = (nx + JBX - 1) / JBX, ty = (ny + JBY - 1) / JBY;
   // ONE_TILE: exactly tile `tile_first` (ensembles); else every CTA-strided tile
   const int t_end = ONE_TILE ? tile_first + 1 : tx * ty;

@@ -57,3 +57,34 @@ def test_noalloc_matches_handle_solver_twice(gpu):
         assert (k, rc) == (k_ref, rc_ref), call
         assert np.array_equal(sol.cpu().numpy(), ref), call
     s.close()
+
+
+@pytest.mark.gpu
+def test_noalloc_arrays_off_16_byte_boundaries(gpu):
+    # Caller arrays that start 8 bytes past a 16-byte boundary (views one double into
+    # a larger buffer): the solve must take its 8-byte copy path and still agree
+    # with the handle solver bit for bit.
+    import torch
+    nx, ny, block = 96, 80, 4
+    N = nx * ny
+    s = swm.Solver(nx=nx, ny=ny, x0=(0.0, 0.0), x1=(1.0, 1.0), solver="stencil",
+                   jacobi_block=block)
+    dev = torch.device("cuda", 0)
+    mass, diag, rhs = patankar_system(N, 21)
+    ref, k_ref, rc_ref = s.debug_jacobi(mass.reshape(-1), diag, rhs)
+
+    def offset_view(host):
+        buf = torch.zeros(N + 1, dtype=torch.float64, device=dev)
+        buf[1:] = torch.from_numpy(np.ascontiguousarray(host)).to(dev)
+        view = buf[1:]
+        assert view.data_ptr() % 16 == 8
+        return buf, view
+
+    keep = [offset_view(mass[:, k]) for k in (0, 1, 3, 4)]
+    keep += [offset_view(diag), offset_view(rhs), offset_view(np.full(N, np.nan))]
+    views = [v for _, v in keep]
+    torch.cuda.synchronize()
+    k, rc = swm.jacobi_noalloc(nx, ny, *[v.data_ptr() for v in views], block=block)
+    assert (k, rc) == (k_ref, rc_ref)
+    assert np.array_equal(views[-1].cpu().numpy(), ref)
+    s.close()
