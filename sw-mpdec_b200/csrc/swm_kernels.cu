@@ -69,6 +69,12 @@ __device__ __forceinline__ bool limbs_le(unsigned long long s2, unsigned long lo
   return s0 <= t[2];
 }
 
+// Approximate value of a limb sum (2^-100 units) for planning only.
+__device__ __forceinline__ double limbs_value(unsigned long long s2, unsigned long long s1,
+                                              unsigned long long s0) {
+  return (double)s2 * 0x1p-20 + (double)s1 * 0x1p-60 + (double)s0 * 0x1p-100;
+}
+
 __device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
@@ -766,10 +772,18 @@ __global__ void __launch_bounds__(JNT, 2) jacobi_kernel(const JacobiArgs a) {
   bool first = true, zero_result = false, maxhit = false;
   int k = 0, final_k = 0;
   const int blk = CSR ? 1 : (a.block < 1 ? 1 : (a.block > TB ? TB : a.block));
+  // Pass planning: a pass costs mostly its tile loads, so a pass that overshoots the
+  // stop (and is redone) or runs sweeps past it is wasted.  After each pass the
+  // residual ratio of its last two sweeps extrapolates the sweeps still needed, and
+  // the next pass is sized to that.  Iterates and stop indices do not depend on the
+  // pass lengths (every sweep's residual is summed and checked in order).
+  int plan = blk;
+  double r_prev = -1.0;
+  const double thresh_d = limbs_value(a.thresh[0], a.thresh[1], a.thresh[2]);
   Acc acc;
   acc_zero(acc);
   for (;;) {
-    int Tp = blk;
+    int Tp = plan;
     if (a.maxiter - k < Tp) Tp = a.maxiter - k;
     if (Tp < 1) Tp = 1;
     for (int q = threadIdx.x; q < (kMaxBlock + 1) * 3; q += blockDim.x) (&s_acc[0][0])[q] = 0ull;
@@ -834,6 +848,18 @@ __global__ void __launch_bounds__(JNT, 2) jacobi_kernel(const JacobiArgs a) {
       }
       result = xout;
       break;
+    }
+    if (!CSR) {
+      const double rT = limbs_value(s_tot[Tp][0], s_tot[Tp][1], s_tot[Tp][2]);
+      const double rP =
+          Tp >= 2 ? limbs_value(s_tot[Tp - 1][0], s_tot[Tp - 1][1], s_tot[Tp - 1][2]) : r_prev;
+      r_prev = rT;
+      plan = blk;
+      if (rP > 0. && rT > 0. && rT < rP && thresh_d > 0.) {
+        const double need = log(thresh_d / rT) / log(rT / rP);
+        if (need > 0. && need < (double)blk) plan = (int)ceil(need);
+      }
+      if (plan < 1) plan = 1;
     }
     k += Tp;
     if (k >= a.maxiter) {
