@@ -75,6 +75,20 @@ __device__ __forceinline__ double limbs_value(unsigned long long s2, unsigned lo
   return (double)s2 * 0x1p-20 + (double)s1 * 0x1p-60 + (double)s0 * 0x1p-100;
 }
 
+// Sweeps of the next pass: a pass costs mostly its tile loads, so one that runs
+// past the stop (or is redone) is wasted.  The residual ratio of the last two
+// sweeps (rT after rP) extrapolates the sweeps still needed to reach the threshold;
+// the next pass runs that many, at most blk.  Iterates and stop indices do not
+// depend on pass lengths: every sweep's residual is summed and checked in order.
+__device__ __forceinline__ int plan_sweeps(double rT, double rP, double thresh_d, int blk) {
+  int plan = blk;
+  if (rP > 0. && rT > 0. && rT < rP && thresh_d > 0.) {
+    const double need = log(thresh_d / rT) / log(rT / rP);
+    if (need > 0. && need < (double)blk) plan = (int)ceil(need);
+  }
+  return plan < 1 ? 1 : plan;
+}
+
 __device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
@@ -772,12 +786,7 @@ __global__ void __launch_bounds__(JNT, 2) jacobi_kernel(const JacobiArgs a) {
   bool first = true, zero_result = false, maxhit = false;
   int k = 0, final_k = 0;
   const int blk = CSR ? 1 : (a.block < 1 ? 1 : (a.block > TB ? TB : a.block));
-  // Pass planning: a pass costs mostly its tile loads, so a pass that overshoots the
-  // stop (and is redone) or runs sweeps past it is wasted.  After each pass the
-  // residual ratio of its last two sweeps extrapolates the sweeps still needed, and
-  // the next pass is sized to that.  Iterates and stop indices do not depend on the
-  // pass lengths (every sweep's residual is summed and checked in order).
-  int plan = blk;
+  int plan = blk;  // sweeps of the next pass (plan_sweeps)
   double r_prev = -1.0;
   const double thresh_d = limbs_value(a.thresh[0], a.thresh[1], a.thresh[2]);
   Acc acc;
@@ -854,12 +863,7 @@ __global__ void __launch_bounds__(JNT, 2) jacobi_kernel(const JacobiArgs a) {
       const double rP =
           Tp >= 2 ? limbs_value(s_tot[Tp - 1][0], s_tot[Tp - 1][1], s_tot[Tp - 1][2]) : r_prev;
       r_prev = rT;
-      plan = blk;
-      if (rP > 0. && rT > 0. && rT < rP && thresh_d > 0.) {
-        const double need = log(thresh_d / rT) / log(rT / rP);
-        if (need > 0. && need < (double)blk) plan = (int)ceil(need);
-      }
-      if (plan < 1) plan = 1;
+      plan = plan_sweeps(rT, rP, thresh_d, blk);
     }
     k += Tp;
     if (k >= a.maxiter) {
@@ -1017,7 +1021,16 @@ __device__ void batch_decide(const JacobiBatchArgs& a, int blk, int* s_cnt) {
           S->result = xout_id(cur);
         } else {
           S->cur = xout_id(cur);
-          S->Tp = (d.maxiter - k < blk) ? d.maxiter - k : blk;
+          const double rT = limbs_value(__ldcg(&S->acc[Tp][0]), __ldcg(&S->acc[Tp][1]),
+                                        __ldcg(&S->acc[Tp][2]));
+          const double rP = Tp >= 2 ? limbs_value(__ldcg(&S->acc[Tp - 1][0]),
+                                                  __ldcg(&S->acc[Tp - 1][1]),
+                                                  __ldcg(&S->acc[Tp - 1][2]))
+                                    : __ldcg(&S->r_prev);
+          S->r_prev = rT;
+          const int plan =
+              plan_sweeps(rT, rP, limbs_value(d.thresh[0], d.thresh[1], d.thresh[2]), blk);
+          S->Tp = (d.maxiter - k < plan) ? d.maxiter - k : plan;
         }
       }
     }
@@ -1053,6 +1066,7 @@ __global__ void __launch_bounds__(JNT, 2) jacobi_batch_kernel(const JacobiBatchA
     S->result = 0;
     S->final_k = 0;
     S->maxhit = 0;
+    S->r_prev = -1.0;
     for (int q = 0; q < (kMaxBlock + 1) * 3; ++q) (&S->acc[0][0])[q] = 0ull;
   }
   if (!grid_barrier(a.ctl, a.spin_limit, &s_ok)) return;

@@ -106,6 +106,7 @@ struct JacBatchState {
   int final_k;
   int maxhit;
   int pad;
+  double r_prev;  // residual sum of the last sweep of the previous pass (pass planning)
   unsigned long long acc[kMaxBlock + 1][3];
 };
 struct JacBatchCtl {
