@@ -786,7 +786,8 @@ __global__ void __launch_bounds__(JNT, 2) jacobi_kernel(const JacobiArgs a) {
   bool first = true, zero_result = false, maxhit = false;
   int k = 0, final_k = 0;
   const int blk = CSR ? 1 : (a.block < 1 ? 1 : (a.block > TB ? TB : a.block));
-  int plan = blk;  // sweeps of the next pass (plan_sweeps)
+  int plan = blk;            // sweeps of the next pass (plan_sweeps)
+  bool expect_stop = false;  // the residual decay reaches the threshold within it
   double r_prev = -1.0;
   const double thresh_d = limbs_value(a.thresh[0], a.thresh[1], a.thresh[2]);
   Acc acc;
@@ -864,6 +865,8 @@ __global__ void __launch_bounds__(JNT, 2) jacobi_kernel(const JacobiArgs a) {
           Tp >= 2 ? limbs_value(s_tot[Tp - 1][0], s_tot[Tp - 1][1], s_tot[Tp - 1][2]) : r_prev;
       r_prev = rT;
       plan = plan_sweeps(rT, rP, thresh_d, blk);
+      expect_stop = rP > 0. && rT > 0. && rT < rP && thresh_d > 0. &&
+                    log(thresh_d / rT) / log(rT / rP) <= (double)blk;
     }
     k += Tp;
     if (k >= a.maxiter) {
@@ -872,8 +875,12 @@ __global__ void __launch_bounds__(JNT, 2) jacobi_kernel(const JacobiArgs a) {
       result = xout;
       break;
     }
+    // the next pass writes the other ping-pong buffer, or, when it is expected to be
+    // the last, the destination itself (unless that is the rhs or holds xin), which
+    // saves copying the result there
     xin = xout;
-    xout = (xout == a.xa) ? a.xb : a.xa;
+    xout = (xin == a.xa) ? a.xb : a.xa;
+    if (expect_stop && a.out != a.b && a.out != xin) xout = a.out;
   }
   // deliver the final iterate (haVec of the reference) to its destination
   const int n = a.nx * a.ny;
