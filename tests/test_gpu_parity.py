@@ -138,6 +138,21 @@ def test_steps_exact_bitwise_wide(gpu, name):
     assert list(s.stats()["jacobi_iters"][:13]) == list(o.last_jacobi_iters()[:13])
 
 
+@pytest.mark.parametrize("maxiter", [1, 2, 3, 5, 6, 7, 9, 1000])
+@pytest.mark.parametrize("block", [2, 4])
+def test_jacobi_planned_passes_vs_maxiter(gpu, maxiter, block):
+    # passes are sized from the residual decay and may write the destination
+    # directly; whatever the plan, the iterate, the stop index and the maxIter
+    # warning must be those of the reference's one-sweep-at-a-time loop
+    c, o, s = make_pair(gpu, "vortex", 96, maxiter=maxiter, solver="stencil", block=block)
+    mass, diag, rhs = random_patankar_system(96 * 96, 17)
+    ref, k_ref = o.jacobi(mass, diag, rhs)
+    got, k, rc = s.debug_jacobi(mass, diag, rhs)
+    assert k == k_ref
+    assert rc == (1 if k_ref == maxiter else 0)
+    assert np.array_equal(got, ref)
+
+
 def test_jacobi_maxiter_warning(gpu):
     c, o, s = make_pair(gpu, "vortex", 40, maxiter=3, solver="stencil", block=2)
     mass, diag, rhs = random_patankar_system(40 * 40, 5)
