@@ -74,6 +74,9 @@ struct swm_solver {
   double* fym[4] = {};
   // Patankar system
   double *cS = nullptr, *cW = nullptr, *cE = nullptr, *cN = nullptr, *cD = nullptr;
+  // stencil mPDeC5: the systems of substeps 3 and 4 when a correction iteration's
+  // three substeps are assembled in one launch ([q][S, W, E, N, D], q = m - 3)
+  double* cset[2][5] = {};
   double *csr_mass = nullptr, *csr_diag = nullptr;
   int *rowstart = nullptr, *cols = nullptr;
   double *xa = nullptr, *xb = nullptr, *rhs_compat = nullptr;
@@ -384,8 +387,13 @@ static int enqueue_step(swm_solver* s) {
   CK(launch_rhs(s, make_rhs_args(s, s->h, s->hu, s->hv, 0)));
   prof_mark(s, -1);
   int solve = 0;
+  // the three substeps of an mPDeC5 correction iteration depend only on the previous
+  // iteration, so (split and FMA forms, stencil layout) they are assembled in one
+  // launch into three systems, then solved one after another
+  const bool fused = !csr && ms == 4 && fast_patankar(s->p) && s->cset[1][4] != nullptr;
   for (int k = 1; k <= kc; ++k) {
     const int mlo = (k == kc) ? ms : 2;
+    const bool fuse_k = fused && k < kc;
     for (int m = mlo; m <= ms; ++m) {
       AssembleArgs aa{};
       aa.nx = s->nx;
@@ -421,9 +429,35 @@ static int enqueue_step(swm_solver* s) {
       aa.fast = fast_patankar(s->p) ? 1 : 0;
       aa.inv_dx = 1.0 / s->gr.dx;
       aa.inv_dy = 1.0 / s->gr.dy;
-      prof_mark(s, 1);
-      CK(launch_assemble(aa, csr, s->stream));
-      prof_mark(s, -1);
+      // substep m's system: the first set, or for a fused iteration the m-th
+      double* sys[5] = {s->cS, s->cW, s->cE, s->cN, s->cD};
+      if (fuse_k && m > 2)
+        for (int c = 0; c < 5; ++c) sys[c] = s->cset[m - 3][c];
+      if (!fuse_k) {
+        prof_mark(s, 1);
+        CK(launch_assemble(aa, csr, s->stream));
+        prof_mark(s, -1);
+      } else if (m == 2) {
+        AssembleMultiArgs ma{};
+        ma.base = aa;
+        ma.nm = 3;
+        for (int q = 0; q < 3; ++q) {
+          const int mq = 2 + q;
+          ma.m[q] = mq;
+          for (int r = 0; r < 4; ++r) ma.theta[q][r] = kTheta5[mq - 1][r];
+          ma.hu_out[q] = s->hum[mq - 1];
+          ma.hv_out[q] = s->hvm[mq - 1];
+          double* const* set = q == 0 ? nullptr : s->cset[q - 1];
+          ma.cS[q] = q == 0 ? s->cS : set[0];
+          ma.cW[q] = q == 0 ? s->cW : set[1];
+          ma.cE[q] = q == 0 ? s->cE : set[2];
+          ma.cN[q] = q == 0 ? s->cN : set[3];
+          ma.cD[q] = q == 0 ? s->cD : set[4];
+        }
+        prof_mark(s, 1);
+        CK(launch_assemble_multi(ma, s->stream));
+        prof_mark(s, -1);
+      }
       JacobiArgs ja{};
       ja.nx = s->nx;
       ja.ny = s->ny;
@@ -431,11 +465,11 @@ static int enqueue_step(swm_solver* s) {
       ja.maxiter = s->p.jacobi_maxiter;
       fill_thresh(s, ja.thresh);
       ja.b = compat ? s->rhs_compat : s->h;
-      ja.cS = s->cS;
-      ja.cW = s->cW;
-      ja.cE = s->cE;
-      ja.cN = s->cN;
-      ja.cD = s->cD;
+      ja.cS = sys[0];
+      ja.cW = sys[1];
+      ja.cE = sys[2];
+      ja.cN = sys[3];
+      ja.cD = sys[4];
       ja.rowstart = s->rowstart;
       ja.cols = s->cols;
       ja.mass = s->csr_mass;
@@ -594,6 +628,9 @@ int swm_create(const swm_params* p, swm_handle* out) {
     AL(s->cE, N);
     AL(s->cN, N);
     AL(s->cD, N);
+    if (p->timescheme == 5 && fast_patankar(*p))
+      for (int q = 0; q < 2; ++q)
+        for (int c = 0; c < 5; ++c) AL(s->cset[q][c], N);
   }
   AL(s->xa, N);
   AL(s->xb, N);

@@ -253,8 +253,34 @@ __device__ __forceinline__ double hp_read(const AssembleArgs& a, int m, int i, i
   return a.hp[m][(size_t)j * a.nx + i];
 }
 
-// One cell of the combination + assembly.  Every input is loaded before any
-// arithmetic (MS stages unrolled), so all of a thread's loads are in flight together.
+// Inputs of one cell shared by every substep m of a correction iteration.
+template <int MS>
+struct CellIn {
+  double dt, fu[MS], fv[MS], fl[4][MS], hu_n, hv_n;
+};
+
+template <int MS>
+__device__ __forceinline__ void load_cell(const AssembleArgs& a, size_t k, size_t kx, CellIn<MS>& c) {
+  c.dt = *a.dt;
+#pragma unroll
+  for (int r = 0; r < MS; ++r) {
+    c.fu[r] = a.fu[r][k];
+    c.fv[r] = a.fv[r][k];
+    c.fl[0][r] = a.fym[r][k];            // S face, oriented into the cell
+    c.fl[1][r] = a.fxm[r][kx];           // W
+    c.fl[2][r] = -a.fxm[r][kx + 1];      // E
+    c.fl[3][r] = -a.fym[r][k + a.nx];    // N
+  }
+  c.hu_n = a.hu_n[k];
+  c.hv_n = a.hv_n[k];
+}
+
+// Outputs of one substep m: Ua(m, 2:3) and its Patankar system (stencil or CSR).
+struct StageOut {
+  double *hu, *hv, *cS, *cW, *cE, *cN, *cD;
+};
+
+// Combination + assembly of substep m (1-based) for one cell from its loaded inputs.
 //  exact: the reference's branches and operation order; each quotient correctly
 //         rounded (div_rn) from RN(1/len) and one RN(1/den(h)) per depth, i.e. equal
 //         to the division it replaces;
@@ -262,38 +288,35 @@ __device__ __forceinline__ double hp_read(const AssembleArgs& a, int m, int i, i
 //         by 1/len (split and FMA forms).  For a face flux f only one of
 //         P = max(f,0)/len and D = -min(f,0)/len is non-zero; the zero one adds an
 //         exact zero, which leaves Mass/Diagonal unchanged.
-template <bool FAST, int MS>
-__device__ __forceinline__ void assemble_cell(const AssembleArgs& a, bool csr, const int i,
-                                              const int j) {
-  const int nx = a.nx, ny = a.ny;
-  const size_t k = (size_t)j * nx + i, kx = (size_t)j * (nx + 1) + i;
+// hp(m) of the cell and of its S, W, E, N neighbours (m 1-based).
+__device__ __forceinline__ void load_hp(const AssembleArgs& a, int m1, int i, int j, double& hK,
+                                        double (&hL)[4]) {
+  const int nx = a.nx, ny = a.ny, m = m1 - 1;
   const int im = i == 0 ? nx - 1 : i - 1, ip = i == nx - 1 ? 0 : i + 1;
   const int jm = j == 0 ? ny - 1 : j - 1, jp = j == ny - 1 ? 0 : j + 1;
-  // ---- loads ----
-  const double dt = *a.dt;
-  double fu[MS], fv[MS], fl[4][MS];
-#pragma unroll
-  for (int r = 0; r < MS; ++r) {
-    fu[r] = a.fu[r][k];
-    fv[r] = a.fv[r][k];
-    fl[0][r] = a.fym[r][k];        // S face, oriented into the cell
-    fl[1][r] = a.fxm[r][kx];       // W
-    fl[2][r] = -a.fxm[r][kx + 1];  // E
-    fl[3][r] = -a.fym[r][k + nx];  // N
-  }
-  const int m = a.m - 1;
-  const double hK = hp_read(a, m, i, j);
-  const double hL[4] = {hp_read(a, m, i, jm), hp_read(a, m, im, j), hp_read(a, m, ip, j),
-                        hp_read(a, m, i, jp)};
-  double au = a.hu_n[k], av = a.hv_n[k];
+  hK = hp_read(a, m, i, j);
+  hL[0] = hp_read(a, m, i, jm);
+  hL[1] = hp_read(a, m, im, j);
+  hL[2] = hp_read(a, m, ip, j);
+  hL[3] = hp_read(a, m, i, jp);
+}
+
+template <bool FAST, int MS>
+__device__ __forceinline__ void assemble_stage(const AssembleArgs& a, bool csr, int i, int j,
+                                               const CellIn<MS>& c, const double hK,
+                                               const double (&hL)[4], const double* theta,
+                                               const StageOut& o) {
+  const size_t k = (size_t)j * a.nx + i;
+  const double dt = c.dt;
+  double au = c.hu_n, av = c.hv_n;
   // ---- explicit momentum (timediscretization.f90:539-543) ----
 #pragma unroll
   for (int r = 0; r < MS; ++r) {
-    au = au + dt * a.theta[r] * fu[r];
-    av = av + dt * a.theta[r] * fv[r];
+    au = au + dt * theta[r] * c.fu[r];
+    av = av + dt * theta[r] * c.fv[r];
   }
-  a.hu_out[k] = au;
-  a.hv_out[k] = av;
+  o.hu[k] = au;
+  o.hv[k] = av;
   // ---- Patankar weights (timediscretization.f90:795-885) ----
   double M[4] = {0., 0., 0., 0.};
   double D = 1.;
@@ -306,16 +329,16 @@ __device__ __forceinline__ void assemble_cell(const AssembleArgs& a, bool csr, c
     const double h = hL[nb], denL = patankar_den(h), rdenL = __drcp_rn(denL);
 #pragma unroll
     for (int r = 0; r < MS; ++r) {
-      const double f = fl[nb][r], th = a.theta[r];
+      const double f = c.fl[nb][r], th = theta[r];
       if (FAST) {
         const double wL = h >= kMinDepth ? (2. * h) * rdenL : 0.;
-        const double c = dt * th, P = dmax(f, 0.) * ilen, Q = dmax(-f, 0.) * ilen;
+        const double cc = dt * th, P = dmax(f, 0.) * ilen, Q = dmax(-f, 0.) * ilen;
         if (th > 0.) {
-          M[nb] = M[nb] - c * (P * wL);
-          D = D + c * (Q * wK);
+          M[nb] = M[nb] - cc * (P * wL);
+          D = D + cc * (Q * wK);
         } else {
-          D = D - c * (P * wK);
-          M[nb] = M[nb] + c * (Q * wL);
+          D = D - cc * (P * wK);
+          M[nb] = M[nb] + cc * (Q * wL);
         }
       } else if (f > 0.) {  // production P_KL = f/len
         const double P = div_rn(f, len, ilen);
@@ -348,13 +371,57 @@ __device__ __forceinline__ void assemble_cell(const AssembleArgs& a, bool csr, c
     mv[4] = M[3];
     a.csr_diag[k] = D;
   } else {
-    a.cS[k] = M[0];
-    a.cW[k] = M[1];
-    a.cE[k] = M[2];
-    a.cN[k] = M[3];
-    a.cD[k] = FAST ? __drcp_rn(D) : D;  // the fast stencil solver multiplies by 1/Diagonal
+    o.cS[k] = M[0];
+    o.cW[k] = M[1];
+    o.cE[k] = M[2];
+    o.cN[k] = M[3];
+    o.cD[k] = FAST ? __drcp_rn(D) : D;  // the fast stencil solver multiplies by 1/Diagonal
   }
+}
+
+// One cell of the combination + assembly of substep a.m.  Every shared input is
+// loaded before any arithmetic (MS stages unrolled), so all of a thread's loads are
+// in flight together.
+template <bool FAST, int MS>
+__device__ __forceinline__ void assemble_cell(const AssembleArgs& a, bool csr, const int i,
+                                              const int j) {
+  const size_t k = (size_t)j * a.nx + i, kx = (size_t)j * (a.nx + 1) + i;
+  CellIn<MS> c;
+  load_cell<MS>(a, k, kx, c);
+  double hK, hL[4];
+  load_hp(a, a.m, i, j, hK, hL);
+  const StageOut o{a.hu_out, a.hv_out, a.cS, a.cW, a.cE, a.cN, a.cD};
+  assemble_stage<FAST, MS>(a, csr, i, j, c, hK, hL, a.theta, o);
   if (a.rhs_out) a.rhs_out[k] = hp_read(a, 0, i, j);  // rhs = hp(1,.) (timediscretization.f90:887)
+}
+
+// The three substeps of one mPDeC5 correction iteration in one pass (split and FMA
+// forms, stencil layout): the stage RHS planes, face fluxes and U^n momentum are
+// read once for all of them; hp(m) and the outputs are per substep.  Every load is
+// issued before the arithmetic.  Each substep's arithmetic is that of
+// assemble_kernel<true, 4>, so the results are identical.
+__global__ void __launch_bounds__(128, 4) assemble_multi_kernel(const AssembleMultiArgs a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y;
+  if (i >= a.base.nx || j >= a.base.ny) return;
+  const size_t k = (size_t)j * a.base.nx + i, kx = (size_t)j * (a.base.nx + 1) + i;
+  CellIn<4> c;
+  load_cell<4>(a.base, k, kx, c);
+  double hK[kMaxFusedStages], hL[kMaxFusedStages][4];
+#pragma unroll
+  for (int q = 0; q < kMaxFusedStages; ++q) load_hp(a.base, a.m[q], i, j, hK[q], hL[q]);
+#pragma unroll
+  for (int q = 0; q < kMaxFusedStages; ++q) {
+    const StageOut o{a.hu_out[q], a.hv_out[q], a.cS[q], a.cW[q], a.cE[q], a.cN[q], a.cD[q]};
+    assemble_stage<true, 4>(a.base, false, i, j, c, hK[q], hL[q], a.theta[q], o);
+  }
+}
+
+cudaError_t launch_assemble_multi(const AssembleMultiArgs& a, cudaStream_t s) {
+  if (a.nm != kMaxFusedStages || a.base.msteps != 4 || !a.base.fast) return cudaErrorInvalidValue;
+  dim3 blk(128), grd((a.base.nx + 127) / 128, a.base.ny);
+  assemble_multi_kernel<<<grd, blk, 0, s>>>(a);
+  return cudaGetLastError();
 }
 
 template <bool FAST, int MS>

@@ -57,6 +57,24 @@ struct AssembleArgs {
   double inv_dx, inv_dy;
 };
 
+// Substeps m of one mPDeC5 correction iteration assembled in one launch (stencil
+// layout): `base` carries the shared inputs (stage RHS slots, face fluxes, hp, U^n
+// momentum, dt, grid); per substep its number, weights and output planes.
+constexpr int kMaxFusedStages = 3;
+struct AssembleMultiArgs {
+  AssembleArgs base;
+  int nm;
+  int m[kMaxFusedStages];  // 1-based substeps
+  double theta[kMaxFusedStages][4];
+  double* hu_out[kMaxFusedStages];
+  double* hv_out[kMaxFusedStages];
+  double* cS[kMaxFusedStages];
+  double* cW[kMaxFusedStages];
+  double* cE[kMaxFusedStages];
+  double* cN[kMaxFusedStages];
+  double* cD[kMaxFusedStages];
+};
+
 struct JacobiArgs {
   int nx, ny;
   int solve_idx;          // slot in ctl->iters
@@ -150,6 +168,7 @@ size_t rhs_smem_bytes(int mode);
 
 cudaError_t launch_dt(const DtArgs& a, cudaStream_t s);
 cudaError_t launch_assemble(const AssembleArgs& a, bool csr, cudaStream_t s);
+cudaError_t launch_assemble_multi(const AssembleMultiArgs& a, cudaStream_t s);
 cudaError_t launch_jacobi(const JacobiArgs& a, bool csr, int grid_blocks, cudaStream_t s);
 int jacobi_grid_blocks(bool csr, int block, int device, bool recip = false);
 cudaError_t launch_ghosted_to_planes(const double* G, int nx, int ny, double* h, double* hu,
