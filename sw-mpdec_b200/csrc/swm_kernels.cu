@@ -284,10 +284,11 @@ struct StageOut {
 //  exact: the reference's branches and operation order; each quotient correctly
 //         rounded (div_rn) from RN(1/len) and one RN(1/den(h)) per depth, i.e. equal
 //         to the division it replaces;
-//  FAST : weights w(h) = 2h/den(h) from one reciprocal per depth and P, D entries
-//         by 1/len (split and FMA forms).  For a face flux f only one of
-//         P = max(f,0)/len and D = -min(f,0)/len is non-zero; the zero one adds an
-//         exact zero, which leaves Mass/Diagonal unchanged.
+//  FAST : weights w(h) = 2h/den(h) from one reciprocal per depth, 1/len folded into
+//         them, dt theta_r formed once and every term added by a fused
+//         multiply-add (split and FMA forms; the batched assembly shares this code,
+//         so ensemble members match single grids).  For a face flux f only one of
+//         max(f,0) and max(-f,0) is non-zero; the zero one adds an exact zero.
 // hp(m) of the cell and of its S, W, E, N neighbours (m 1-based).
 __device__ __forceinline__ void load_hp(const AssembleArgs& a, int m1, int i, int j, double& hK,
                                         double (&hL)[4]) {
@@ -308,55 +309,79 @@ __device__ __forceinline__ void assemble_stage(const AssembleArgs& a, bool csr, 
                                                const StageOut& o) {
   const size_t k = (size_t)j * a.nx + i;
   const double dt = c.dt;
-  double au = c.hu_n, av = c.hv_n;
-  // ---- explicit momentum (timediscretization.f90:539-543) ----
-#pragma unroll
-  for (int r = 0; r < MS; ++r) {
-    au = au + dt * theta[r] * c.fu[r];
-    av = av + dt * theta[r] * c.fv[r];
-  }
-  o.hu[k] = au;
-  o.hv[k] = av;
-  // ---- Patankar weights (timediscretization.f90:795-885) ----
   double M[4] = {0., 0., 0., 0.};
   double D = 1.;
-  const double denK = patankar_den(hK), rdenK = __drcp_rn(denK);
-  const double wK = (FAST && hK >= kMinDepth) ? (2. * hK) * rdenK : 0.;
+  if constexpr (FAST) {
+    // the same sums with dt theta_r formed once, 1/len folded into the depth
+    // weights, and each term added by one fused multiply-add
+    double cr[MS];
 #pragma unroll
-  for (int nb = 0; nb < 4; ++nb) {
-    const bool ydir = (nb == 0 || nb == 3);
-    const double len = ydir ? a.dy : a.dx, ilen = ydir ? a.inv_dy : a.inv_dx;
-    const double h = hL[nb], denL = patankar_den(h), rdenL = __drcp_rn(denL);
+    for (int r = 0; r < MS; ++r) cr[r] = dt * theta[r];
+    double au = c.hu_n, av = c.hv_n;
 #pragma unroll
     for (int r = 0; r < MS; ++r) {
-      const double f = c.fl[nb][r], th = theta[r];
-      if (FAST) {
-        const double wL = h >= kMinDepth ? (2. * h) * rdenL : 0.;
-        const double cc = dt * th, P = dmax(f, 0.) * ilen, Q = dmax(-f, 0.) * ilen;
-        if (th > 0.) {
-          M[nb] = M[nb] - cc * (P * wL);
-          D = D + cc * (Q * wK);
+      au = fma(cr[r], c.fu[r], au);
+      av = fma(cr[r], c.fv[r], av);
+    }
+    o.hu[k] = au;
+    o.hv[k] = av;
+    const double wK = hK >= kMinDepth ? (2. * hK) * __drcp_rn(patankar_den(hK)) : 0.;
+#pragma unroll
+    for (int nb = 0; nb < 4; ++nb) {
+      const double ilen = (nb == 0 || nb == 3) ? a.inv_dy : a.inv_dx;
+      const double h = hL[nb];
+      const double wL = h >= kMinDepth ? (2. * h) * __drcp_rn(patankar_den(h)) : 0.;
+      const double aL = ilen * wL, aK = ilen * wK;
+#pragma unroll
+      for (int r = 0; r < MS; ++r) {
+        const double f = c.fl[nb][r], pf = dmax(f, 0.), qf = dmax(-f, 0.);
+        if (theta[r] > 0.) {
+          M[nb] = fma(-(cr[r] * pf), aL, M[nb]);
+          D = fma(cr[r] * qf, aK, D);
         } else {
-          D = D - cc * (P * wK);
-          M[nb] = M[nb] + cc * (Q * wL);
+          D = fma(-(cr[r] * pf), aK, D);
+          M[nb] = fma(cr[r] * qf, aL, M[nb]);
         }
-      } else if (f > 0.) {  // production P_KL = f/len
-        const double P = div_rn(f, len, ilen);
-        if (th > 0.) {
-          const double pd = h < kMinDepth ? 0. : div_rn(2. * h * P, denL, rdenL);
-          M[nb] = M[nb] - dt * th * pd;
-        } else {
-          const double pd = hK < kMinDepth ? 0. : div_rn(2. * hK * P, denK, rdenK);
-          D = D - dt * th * pd;
-        }
-      } else if (f < 0.) {  // destruction D_KL = -f/len
-        const double Q = div_rn(-f, len, ilen);
-        if (th > 0.) {
-          const double pd = hK < kMinDepth ? 0. : div_rn(2. * hK * Q, denK, rdenK);
-          D = D + dt * th * pd;
-        } else {
-          const double pd = h < kMinDepth ? 0. : div_rn(2. * h * Q, denL, rdenL);
-          M[nb] = M[nb] + dt * th * pd;
+      }
+    }
+  } else {
+    double au = c.hu_n, av = c.hv_n;
+    // ---- explicit momentum (timediscretization.f90:539-543) ----
+  #pragma unroll
+    for (int r = 0; r < MS; ++r) {
+      au = au + dt * theta[r] * c.fu[r];
+      av = av + dt * theta[r] * c.fv[r];
+    }
+    o.hu[k] = au;
+    o.hv[k] = av;
+    // ---- Patankar weights (timediscretization.f90:795-885) ----
+    const double denK = patankar_den(hK), rdenK = __drcp_rn(denK);
+  #pragma unroll
+    for (int nb = 0; nb < 4; ++nb) {
+      const bool ydir = (nb == 0 || nb == 3);
+      const double len = ydir ? a.dy : a.dx, ilen = ydir ? a.inv_dy : a.inv_dx;
+      const double h = hL[nb], denL = patankar_den(h), rdenL = __drcp_rn(denL);
+  #pragma unroll
+      for (int r = 0; r < MS; ++r) {
+        const double f = c.fl[nb][r], th = theta[r];
+        if (f > 0.) {  // production P_KL = f/len
+          const double P = div_rn(f, len, ilen);
+          if (th > 0.) {
+            const double pd = h < kMinDepth ? 0. : div_rn(2. * h * P, denL, rdenL);
+            M[nb] = M[nb] - dt * th * pd;
+          } else {
+            const double pd = hK < kMinDepth ? 0. : div_rn(2. * hK * P, denK, rdenK);
+            D = D - dt * th * pd;
+          }
+        } else if (f < 0.) {  // destruction D_KL = -f/len
+          const double Q = div_rn(-f, len, ilen);
+          if (th > 0.) {
+            const double pd = hK < kMinDepth ? 0. : div_rn(2. * hK * Q, denK, rdenK);
+            D = D + dt * th * pd;
+          } else {
+            const double pd = h < kMinDepth ? 0. : div_rn(2. * h * Q, denL, rdenL);
+            M[nb] = M[nb] + dt * th * pd;
+          }
         }
       }
     }
