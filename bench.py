@@ -75,17 +75,27 @@ class ClockSampler:
         self.device = device
         self.proc = None
         self.lines = []
+        self.first = 0
 
     def start(self):
+        """Start sampling every 25 ms; return once the first sample has arrived, so
+        that a short timed region is covered from its beginning."""
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "25"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            t_end = time.time() + 5.0
+            while not self.lines and time.time() < t_end and self.proc.poll() is None:
+                time.sleep(0.01)
         except OSError:
             self.proc = None
+
+    def mark(self):
+        """The timed region starts now: earlier samples are not counted."""
+        self.first = len(self.lines)
 
     def _read(self):
         for line in self.proc.stdout:
@@ -101,7 +111,7 @@ class ClockSampler:
             self.proc.kill()
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        for ln in self.lines[self.first:]:
             parts = [p.strip() for p in ln.split(",")]
             if len(parts) < 7:
                 continue
@@ -124,13 +134,16 @@ def make_solver(swm, c, precision, solver="stencil", block=4, device=0):
                       jacobi_block=block, device=device)
 
 
-def timed_steps(s, torch, steps, warmup):
-    """W untimed steps, then K steps bracketed by CUDA events on the library stream."""
+def timed_steps(s, torch, steps, warmup, on_start=None):
+    """W untimed steps, then K steps bracketed by CUDA events on the library stream;
+    on_start() is called just before the first timed step."""
     for _ in range(warmup):
         s.step(0.0, s.timestep())
     st = torch.cuda.ExternalStream(s.stream())
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
+    if on_start:
+        on_start()
     e0.record(st)
     iters = 0
     for _ in range(steps):
@@ -256,7 +269,8 @@ def main():
         sampler = ClockSampler(local) if prec == "split" else None
         if sampler:
             sampler.start()
-        ms, iters = timed_steps(s, torch, args.steps, args.warmup)
+        ms, iters = timed_steps(s, torch, args.steps, args.warmup,
+                                on_start=sampler.mark if sampler else None)
         if sampler:
             clocks = sampler.stop()
         barrier()
