@@ -44,7 +44,7 @@ PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
 NCU_TRAFFIC_2048 = {
     "rhs": (101284864.0 + 92335104.0, "profiles/rhs_split_island2048.md"),
     "patankar_assemble": (None, "profiles/assemble_split_island2048.md"),  # k = 1 launch only
-    "jacobi": (464084224.0 + 66940672.0, "profiles/jacobi_stencil4_split_island2048.md"),
+    "jacobi": (437117696.0 + 59626752.0, "profiles/jacobi_stencil4_split_island2048.md"),
 }
 
 # Algorithmic bytes per cell-step of the whole mPDeC5 step: every phase reads its
