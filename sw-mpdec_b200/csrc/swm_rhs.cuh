@@ -289,7 +289,8 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const i
       sFX[(2 * TY + rr) * (TX + 1) + ff] = s2;
     };
     face_pass<TY * (TX + 1), NT>(gr, xface, xstore);
-    __syncthreads();
+    // no barrier: the y first sweeps below share this phase (they write sF1, free since
+    // the x second sweeps; this pass reads sW and writes sFX)
   }
 
   // ======================= y direction =======================
@@ -302,7 +303,7 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const i
       // share four of their six values
       static_assert(FH % 2 == 0, "row pairs");
       constexpr int FH2 = FH / 2;
-      for (int it = tid; it < 3 * FH2 * FW; it += NT) {
+      for (int it = NT - 1 - tid; it < 3 * FH2 * FW; it += NT) {  // reversed: balances the x faces
         int cc = it % FW, rest = it / FW, rr = 2 * (rest % FH2), v = rest / FH2;
         // V rows (j0-1+rr)-2 .. +2 -> tile rows rr..rr+4; col (i0-2+cc) -> tile col cc+1
         f2 q[5];
@@ -315,7 +316,7 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const i
         f2_unpack(wp, sTP[(v * FH + rr) * FW + cc], sTP[(v * FH + rr + 1) * FW + cc]);
       }
     } else {
-      for (int it = tid; it < 3 * FH * FW; it += NT) {
+      for (int it = NT - 1 - tid; it < 3 * FH * FW; it += NT) {  // reversed: balances the x faces
         int cc = it % FW, rest = it / FW, rr = rest % FH, v = rest / FH;
         // V rows (j0-1+rr)-2 .. +2 -> tile rows rr..rr+4; col (i0-2+cc) -> tile col cc+1
         double q0 = SV(v, rr, cc + 1), q1 = SV(v, rr + 1, cc + 1), q2 = SV(v, rr + 2, cc + 1),
@@ -391,7 +392,8 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const i
       sFY[(2 * (TY + 1) + fr) * TX + cc] = s2;
     };
     face_pass<(TY + 1) * TX, NT>(gr, yface, ystore);
-    __syncthreads();
+    // no barrier: the source sweeps below share this phase (they write sF1, whose y
+    // first sweeps the y second sweeps have consumed; this pass reads sW, writes sFY)
   }
 
   // ======================= source term (depth only) =======================
@@ -401,7 +403,7 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const i
   if (has_src) {
     if constexpr (MODE == 1) {
       static_assert(TY % 2 == 0, "row pairs");
-      for (int it = tid; it < (TY / 2) * SW_; it += NT) {
+      for (int it = NT - 1 - tid; it < (TY / 2) * SW_; it += NT) {  // reversed: balances the y faces
         int cc = it % SW_, rr = 2 * (it / SW_);
         // U(1) = V(1) = h; rows (j0+rr)-2..+2 -> tile rows rr+1..rr+5; col i0-2+cc -> cc+1
         f2 q[5], w[4];
@@ -415,7 +417,7 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const i
           f2_unpack(w[g], sVt[(g * TY + rr) * SW_ + cc], sVt[(g * TY + rr + 1) * SW_ + cc]);
       }
     } else {
-      for (int it = tid; it < TY * SW_; it += NT) {
+      for (int it = NT - 1 - tid; it < TY * SW_; it += NT) {  // reversed: balances the y faces
         int cc = it % SW_, rr = it / SW_;
         double q0 = SV(0, rr + 1, cc + 1), q1 = SV(0, rr + 2, cc + 1), q2 = SV(0, rr + 3, cc + 1),
                q3 = SV(0, rr + 4, cc + 1), q4 = SV(0, rr + 5, cc + 1);
@@ -425,8 +427,8 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const i
         for (int g = 0; g < 4; ++g) sVt[(g * TY + rr) * SW_ + cc] = w[g];
       }
     }
-    __syncthreads();
   }
+  __syncthreads();  // fluxes and source sweeps complete
 
   // ======================= per-cell epilogue =======================
   for (int it = tid; it < TX * TY; it += NT) {
