@@ -70,8 +70,11 @@ struct RhsSmem {
   static constexpr int nFY = 3 * (TY + 1) * TX;                   // double
   // split form: V also as float pairs hi + lo (hi = fl32(V), lo = fl32(V - hi))
   static constexpr int nVF = std::is_same<T, float>::value ? 2 * nV : 0;  // float
-  static constexpr size_t bytes =
-      sizeof(double) * (nV + nW + nFX + nFY) + sizeof(T) * nF1 + sizeof(float) * nVF;
+  // split form: the source term's y sweeps [4][TY][TX+4] in a buffer of their own, so
+  // they can run in the x second-sweep phase (the FP64 form reuses the first-sweep area)
+  static constexpr int nVt = std::is_same<T, float>::value ? 4 * TY * (TX + 4) : 0;  // float
+  static constexpr size_t bytes = sizeof(double) * (nV + nW + nFX + nFY) + sizeof(T) * nF1 +
+                                  sizeof(float) * (nVF + nVt);
 };
 
 }  // namespace swm
@@ -193,6 +196,30 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const i
     return (sVh[k] - sVh[kc]) + (sVl[k] - sVl[kc]);
   };
 
+  // source term's y sweeps of h at the 4 y Gauss points (split form: own buffer)
+  const bool has_src = gr.bathy > 0;
+  constexpr int SW_ = TX + 4;  // y-sweep columns i0-2..i0+TX+1
+  T* sVt = (MODE == 1) ? reinterpret_cast<T*>(sVl + SM::nV) : sF1;  // [4][TY][TX+4]
+  auto src_sweeps_split = [&]() {
+    if constexpr (MODE == 1) {
+    static_assert(TY % 2 == 0, "row pairs");
+    static_assert(SM::nVt == 4 * TY * SW_, "source sweep buffer");
+    for (int it = NT - 1 - tid; it < (TY / 2) * SW_; it += NT) {  // reversed: fills the last round
+      int cc = it % SW_, rr = 2 * (it / SW_);
+      // U(1) = V(1) = h; rows (j0+rr)-2..+2 -> tile rows rr+1..rr+5; col i0-2+cc -> cc+1
+      f2 q[5], w[4];
+#pragma unroll
+      for (int k = 0; k < 5; ++k)
+        q[k] = f2_pack(dev(0, rr + 1 + k, cc + 1, rr + 3, cc + 1),
+                       dev(0, rr + 2 + k, cc + 1, rr + 4, cc + 1));
+      weno5_second_x2(q[0], q[1], q[2], q[3], q[4], w);
+#pragma unroll
+      for (int g = 0; g < 4; ++g)
+        f2_unpack(w[g], sVt[(g * TY + rr) * SW_ + cc], sVt[(g * TY + rr + 1) * SW_ + cc]);
+    }
+    }
+  };
+
   // ======================= x direction =======================
   {
     constexpr int FW = TX + 2, FH = TY + 4;  // first sweeps: cols i0-1..i0+TX, rows j0-2..j0+TY+1
@@ -272,6 +299,9 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const i
         sW[((0 * 3 + v) * 4 + g) * WC + rr * FW + cc] = wmv[g];
         sW[((1 * 3 + v) * 4 + g) * WC + rr * FW + cc] = wpv[g];
       }
+    }
+    if constexpr (MODE == 1) {  // fills the last, partial round of the second sweeps
+      if (has_src) src_sweeps_split();
     }
     __syncthreads();
     // Rusanov at faces f = i0 .. i0+TX (ff), rows rr; left = WP(cell f-1) (cc = ff), right = WM(f)
@@ -397,26 +427,9 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const i
   }
 
   // ======================= source term (depth only) =======================
-  const bool has_src = gr.bathy > 0;
-  constexpr int SW_ = TX + 4;  // y-sweep columns i0-2..i0+TX+1
-  T* sVt = sF1;                // [4][TY][TX+4]
+  // (the split form's y sweeps ran in the x second-sweep phase)
   if (has_src) {
-    if constexpr (MODE == 1) {
-      static_assert(TY % 2 == 0, "row pairs");
-      for (int it = NT - 1 - tid; it < (TY / 2) * SW_; it += NT) {  // reversed: balances the y faces
-        int cc = it % SW_, rr = 2 * (it / SW_);
-        // U(1) = V(1) = h; rows (j0+rr)-2..+2 -> tile rows rr+1..rr+5; col i0-2+cc -> cc+1
-        f2 q[5], w[4];
-#pragma unroll
-        for (int k = 0; k < 5; ++k)
-          q[k] = f2_pack(dev(0, rr + 1 + k, cc + 1, rr + 3, cc + 1),
-                         dev(0, rr + 2 + k, cc + 1, rr + 4, cc + 1));
-        weno5_second_x2(q[0], q[1], q[2], q[3], q[4], w);
-#pragma unroll
-        for (int g = 0; g < 4; ++g)
-          f2_unpack(w[g], sVt[(g * TY + rr) * SW_ + cc], sVt[(g * TY + rr + 1) * SW_ + cc]);
-      }
-    } else {
+    if constexpr (MODE == 0) {
       for (int it = NT - 1 - tid; it < TY * SW_; it += NT) {  // reversed: balances the y faces
         int cc = it % SW_, rr = it / SW_;
         double q0 = SV(0, rr + 1, cc + 1), q1 = SV(0, rr + 2, cc + 1), q2 = SV(0, rr + 3, cc + 1),
