@@ -160,29 +160,43 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const i
   // Periodic wrap: one conditional add/subtract when the grid is at least one haloed
   // tile wide, the general modulo otherwise.
   const bool wide = nx >= VX && ny >= VY;
-  for (int it = tid; it < VY * VX; it += NT) {
-    int cx = it % VX, cy = it / VX;
-    int gi = i0 - 3 + cx, gj = j0 - 3 + cy;
-    if (wide) {
-      gi += gi < 0 ? nx : (gi >= nx ? -nx : 0);
-      gj += gj < 0 ? ny : (gj >= ny ? -ny : 0);
-    } else {
-      gi = wrap(gi, nx);
-      gj = wrap(gj, ny);
+  constexpr int NLD = (VY * VX + NT - 1) / NT;  // cells per thread; all loads issued first
+  double lh[NLD], lhu[NLD], lhv[NLD];
+#pragma unroll
+  for (int q = 0; q < NLD; ++q) {
+    const int it = tid + q * NT;
+    if (it < VY * VX) {
+      int gi = i0 - 3 + it % VX, gj = j0 - 3 + it / VX;
+      if (wide) {
+        gi += gi < 0 ? nx : (gi >= nx ? -nx : 0);
+        gj += gj < 0 ? ny : (gj >= ny ? -ny : 0);
+      } else {
+        gi = wrap(gi, nx);
+        gj = wrap(gj, ny);
+      }
+      const size_t k = (size_t)gj * nx + gi;
+      lh[q] = a.h[k];
+      lhu[q] = a.hu[k];
+      lhv[q] = a.hv[k];
     }
-    size_t k = (size_t)gj * nx + gi;
-    double h = a.h[k], hu = a.hu[k], hv = a.hv[k], u, v;
+  }
+#pragma unroll
+  for (int q = 0; q < NLD; ++q) {
+    const int it = tid + q * NT;
+    if (it >= VY * VX) break;
+    const int cx = it % VX, cy = it / VX;
+    double h = lh[q], hu = lhu[q], hv = lhv[q], u, v;
     cons_to_prim<EX>(h, hu, hv, u, v);
     sV[(0 * VY + cy) * VX + cx] = h;
     sV[(1 * VY + cy) * VX + cx] = u;
     sV[(2 * VY + cy) * VX + cx] = v;
     if constexpr (MODE == 1) {
-      const double q[3] = {h, u, v};
+      const double qv[3] = {h, u, v};
 #pragma unroll
       for (int w = 0; w < 3; ++w) {
-        const float hi = (float)q[w];
+        const float hi = (float)qv[w];
         sVh[(w * VY + cy) * VX + cx] = hi;
-        sVl[(w * VY + cy) * VX + cx] = (float)(q[w] - (double)hi);
+        sVl[(w * VY + cy) * VX + cx] = (float)(qv[w] - (double)hi);
       }
     }
   }
