@@ -708,7 +708,8 @@ __device__ __forceinline__ void tile_sweeps(const double* sm, double*& xp, doubl
       __syncthreads();
       double* tmp = xp;
       xp = xn;
-      xn = tmp;
+      // a first sweep that read x^0 = b from b's own tile hands over the x0 buffer
+      xn = (tmp == sm + 5 * JTile<TB>::HN) ? const_cast<double*>(sm) + 6 * JTile<TB>::HN : tmp;
       tile_sweeps<TB, T + 1, RECIP>(sm, xp, xn, Tp, cx_lim, cy_lim, acc);
     }
   }
@@ -767,6 +768,8 @@ __device__ void stencil_tiles(const JacobiArgs& a, const double* xin, double* xo
   // 16-byte pairs need an even first column (i0 - TB), an even row pitch and 16-byte
   // aligned arrays (the allocation-free entry takes the caller's pointers as given)
   const bool pairs = (TB % 2 == 0) && !small && (nx % 2 == 0) && arrays_aligned16(a, xin);
+  // first pass: x^0 = b, already in the b tile (sweep 1 reads it there)
+  const bool from_b = xin == a.b;
   const int tx = (nx + JBX - 1) / JBX, ty = (ny + JBY - 1) / JBY;
   // ONE_TILE: exactly tile `tile_first` (ensembles); else every CTA-strided tile
   const int t_end = ONE_TILE ? tile_first + 1 : tx * ty;
@@ -796,7 +799,7 @@ __device__ void stencil_tiles(const JacobiArgs& a, const double* xin, double* xo
           cp_async16(&sN[c], &a.cN[g]);
           cp_async16(&sD[c], &a.cD[g]);
           cp_async16(&sB[c], &a.b[g]);
-          cp_async16(&x0[c], &xin[g]);
+          if (!from_b) cp_async16(&x0[c], &xin[g]);
         }
       }
       cp_async_wait_all();
@@ -816,7 +819,7 @@ __device__ void stencil_tiles(const JacobiArgs& a, const double* xin, double* xo
           sN[c] = a.cN[g];
           sD[c] = a.cD[g];
           sB[c] = a.b[g];
-          x0[c] = __ldcg(&xin[g]);
+          if (!from_b) x0[c] = __ldcg(&xin[g]);
         }
       }
     }
@@ -826,7 +829,7 @@ __device__ void stencil_tiles(const JacobiArgs& a, const double* xin, double* xo
         for (int lx = TB + lane; lx < TB + JBX; lx += 32)
           if (i0 + lx - TB < nx && j0 + ly - TB < ny) acc_put<0>(acc, fabs(0. - sB[ly * HX + lx]));
     }
-    double* xp = x0;
+    double* xp = from_b ? sB : x0;
     double* xn = x1;
     tile_sweeps<TB, 1, RECIP>(sm, xp, xn, Tp, cx_lim, cy_lim, acc);
     for (int ly = TB + warp; ly < TB + JBY; ly += NW) {
