@@ -1320,13 +1320,17 @@ int swm_debug_jacobi(swm_handle s, const double* mass, const double* diag, const
     CK(cudaMemcpy(s->csr_mass, mass, 5 * N * sizeof(double), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(s->csr_diag, diag, N * sizeof(double), cudaMemcpyHostToDevice));
   } else {
+    // the fast solver's planes hold the row divided by its Diagonal and rhs/Diagonal
+    // (the fast assembly writes the same: products with RN(1/D))
+    const bool fast = fast_patankar(s->p);
     std::vector<double> pl(5 * N);
     for (size_t k = 0; k < N; ++k) {
-      pl[k] = mass[5 * k + 0];
-      pl[N + k] = mass[5 * k + 1];
-      pl[2 * N + k] = mass[5 * k + 3];
-      pl[3 * N + k] = mass[5 * k + 4];
-      pl[4 * N + k] = fast_patankar(s->p) ? 1.0 / diag[k] : diag[k];
+      const double r = fast ? 1.0 / diag[k] : 1.0;
+      pl[k] = fast ? mass[5 * k + 0] * r : mass[5 * k + 0];
+      pl[N + k] = fast ? mass[5 * k + 1] * r : mass[5 * k + 1];
+      pl[2 * N + k] = fast ? mass[5 * k + 3] * r : mass[5 * k + 3];
+      pl[3 * N + k] = fast ? mass[5 * k + 4] * r : mass[5 * k + 4];
+      pl[4 * N + k] = fast ? rhs[k] * r : diag[k];
     }
     CK(cudaMemcpy(s->cS, pl.data(), N * sizeof(double), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(s->cW, pl.data() + N, N * sizeof(double), cudaMemcpyHostToDevice));

@@ -257,11 +257,14 @@ __device__ __forceinline__ double hp_read(const AssembleArgs& a, int m, int i, i
 template <int MS>
 struct CellIn {
   double dt, fu[MS], fv[MS], fl[4][MS], hu_n, hv_n;
+  double b;  // FAST: the solve's rhs hp(1,.) (timediscretization.f90:887)
 };
 
-template <int MS>
-__device__ __forceinline__ void load_cell(const AssembleArgs& a, size_t k, size_t kx, CellIn<MS>& c) {
+template <bool FAST, int MS>
+__device__ __forceinline__ void load_cell(const AssembleArgs& a, int i, int j, size_t k, size_t kx,
+                                          CellIn<MS>& c) {
   c.dt = *a.dt;
+  if constexpr (FAST) c.b = hp_read(a, 0, i, j);
 #pragma unroll
   for (int r = 0; r < MS; ++r) {
     c.fu[r] = a.fu[r][k];
@@ -395,12 +398,21 @@ __device__ __forceinline__ void assemble_stage(const AssembleArgs& a, bool csr, 
     mv[3] = M[2];
     mv[4] = M[3];
     a.csr_diag[k] = D;
+  } else if constexpr (FAST) {
+    // the fast stencil solver iterates x = b/D - sum (M/D) x: the row divided by its
+    // Diagonal, the rhs b = hp(1,.) (timediscretization.f90:887) in the D plane
+    const double rD = __drcp_rn(D);
+    o.cS[k] = M[0] * rD;
+    o.cW[k] = M[1] * rD;
+    o.cE[k] = M[2] * rD;
+    o.cN[k] = M[3] * rD;
+    o.cD[k] = c.b * rD;
   } else {
     o.cS[k] = M[0];
     o.cW[k] = M[1];
     o.cE[k] = M[2];
     o.cN[k] = M[3];
-    o.cD[k] = FAST ? __drcp_rn(D) : D;  // the fast stencil solver multiplies by 1/Diagonal
+    o.cD[k] = D;
   }
 }
 
@@ -412,7 +424,7 @@ __device__ __forceinline__ void assemble_cell(const AssembleArgs& a, bool csr, c
                                               const int j) {
   const size_t k = (size_t)j * a.nx + i, kx = (size_t)j * (a.nx + 1) + i;
   CellIn<MS> c;
-  load_cell<MS>(a, k, kx, c);
+  load_cell<FAST, MS>(a, i, j, k, kx, c);
   double hK, hL[4];
   load_hp(a, a.m, i, j, hK, hL);
   const StageOut o{a.hu_out, a.hv_out, a.cS, a.cW, a.cE, a.cN, a.cD};
@@ -431,7 +443,7 @@ __global__ void __launch_bounds__(128, 4) assemble_multi_kernel(const AssembleMu
   if (i >= a.base.nx || j >= a.base.ny) return;
   const size_t k = (size_t)j * a.base.nx + i, kx = (size_t)j * (a.base.nx + 1) + i;
   CellIn<4> c;
-  load_cell<4>(a.base, k, kx, c);
+  load_cell<true, 4>(a.base, i, j, k, kx, c);
   double hK[kMaxFusedStages], hL[kMaxFusedStages][4];
 #pragma unroll
   for (int q = 0; q < kMaxFusedStages; ++q) load_hp(a.base, a.m[q], i, j, hK[q], hL[q]);
@@ -673,9 +685,10 @@ __device__ __forceinline__ void tile_sweep(const double* sm, const double* xp, d
     if (NU % JNT != 0 && u >= NU) break;
     const int ly = T + u / NP, lx = 2 * (P0 + u % NP);
     const int c = ly * HX + lx;
+    // RECIP (split form): the planes hold the row divided by its Diagonal and b/D
     const double2 cS = lds2(sm + c), cW = lds2(sm + HN + c), cE = lds2(sm + 2 * HN + c),
                   cN = lds2(sm + 3 * HN + c), cD = lds2(sm + 4 * HN + c),
-                  cB = lds2(sm + 5 * HN + c);
+                  cB = RECIP ? cD : lds2(sm + 5 * HN + c);
     const double2 xs = lds2(xp + c - HX), xc = lds2(xp + c), xq = lds2(xp + c + HX);
     const double xw = xp[c - 1], xe = xp[c + 2];
     // product = (((S x_S + W x_W) + E x_E) + N x_N); the zero centre slot of the
@@ -688,8 +701,8 @@ __device__ __forceinline__ void tile_sweep(const double* sm, const double* xp, d
     p0 = __dadd_rn(p0, __dmul_rn(cN.x, xq.x));
     p1 = __dadd_rn(p1, __dmul_rn(cN.y, xq.y));
     double2 v;
-    v.x = RECIP ? __dmul_rn(__dsub_rn(cB.x, p0), cD.x) : __ddiv_rn(__dsub_rn(cB.x, p0), cD.x);
-    v.y = RECIP ? __dmul_rn(__dsub_rn(cB.y, p1), cD.y) : __ddiv_rn(__dsub_rn(cB.y, p1), cD.y);
+    v.x = RECIP ? __dsub_rn(cD.x, p0) : __ddiv_rn(__dsub_rn(cB.x, p0), cD.x);
+    v.y = RECIP ? __dsub_rn(cD.y, p1) : __ddiv_rn(__dsub_rn(cB.y, p1), cD.y);
     *reinterpret_cast<double2*>(xn + c) = v;
     if ((unsigned)(ly - TB) < (unsigned)cy_lim) {
       if ((unsigned)(lx - TB) < (unsigned)cx_lim) acc_put<T>(acc, fabs(__dsub_rn(v.x, xc.x)));
@@ -798,7 +811,7 @@ __device__ void stencil_tiles(const JacobiArgs& a, const double* xin, double* xo
           cp_async16(&sE[c], &a.cE[g]);
           cp_async16(&sN[c], &a.cN[g]);
           cp_async16(&sD[c], &a.cD[g]);
-          cp_async16(&sB[c], &a.b[g]);
+          if (!RECIP || from_b) cp_async16(&sB[c], &a.b[g]);  // RECIP: b only for x^0
           if (!from_b) cp_async16(&x0[c], &xin[g]);
         }
       }
@@ -818,7 +831,7 @@ __device__ void stencil_tiles(const JacobiArgs& a, const double* xin, double* xo
           sE[c] = a.cE[g];
           sN[c] = a.cN[g];
           sD[c] = a.cD[g];
-          sB[c] = a.b[g];
+          if (!RECIP || from_b) sB[c] = a.b[g];
           if (!from_b) x0[c] = __ldcg(&xin[g]);
         }
       }

@@ -52,7 +52,8 @@ struct AssembleArgs {
   double* csr_diag;
   double* rhs_out;        // nullable: rhs = hp(1,.) (needed when hp is read through compat2)
   // split form: PATANKAR_DIV from one reciprocal per depth, P/D by 1/dx, and the
-  // stencil diagonal stored as 1/Diagonal (not bit-identical to the reference order)
+  // stencil planes holding the row divided by its Diagonal, the D plane b/Diagonal
+  // (not bit-identical to the reference order)
   int fast;
   double inv_dx, inv_dy;
 };
@@ -97,7 +98,7 @@ struct JacobiArgs {
   double* out;            // final iterate destination
   JacobiCtl* ctl;
   int block;              // sweeps per pass (stencil)
-  int recip;              // stencil: cD holds 1/Diagonal (split form)
+  int recip;              // stencil (split form): S..N hold Mass/Diagonal, cD holds b/Diagonal
   long long spin_limit;   // grid-barrier watchdog
 };
 
