@@ -44,7 +44,7 @@ PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
 NCU_TRAFFIC_2048 = {
     "rhs": (101286912.0 + 94110208.0, "profiles/rhs_split_island2048.md"),
     "patankar_assemble": (None, "profiles/assemble_split_island2048.md"),  # k = 1 launch only
-    "jacobi": (437117696.0 + 59626752.0, "profiles/jacobi_stencil4_split_island2048.md"),
+    "jacobi": (403459328.0 + 58311680.0, "profiles/jacobi_stencil4_split_island2048.md"),
 }
 
 # Algorithmic bytes per cell-step of the whole mPDeC5 step: every phase reads its
