@@ -319,75 +319,120 @@ __device__ __forceinline__ f2 rcp2(f2 a) {
   f2_unpack(a, lo, hi);
   return f2_pack(rcp_(lo), rcp_(hi));
 }
-// c1 x1 + c2 x2 + c3 x3 with scalar coefficients
-__device__ __forceinline__ f2 lin3(float c1, f2 x1, float c2, f2 x2, float c3, f2 x3) {
-  return fma2(f2_splat(c3), x3, fma2(f2_splat(c2), x2, mul2(f2_splat(c1), x1)));
-}
+// Packed WENO5 in the candidate-quadratic form.  On the cell xi in [-1/2, 1/2] the
+// quadratic whose cell averages match candidate stencil k is
+//   p_1(xi) = q0 + hx r_1 + tau s_1,  p_2 = q0 - hx r_2 + tau s_2,  p_3 = q0 - hx r_3 + tau s_3,
+// hx = xi/2, tau = (xi^2 - 1/12)/2, with the second differences s_1 = qm2 - 2qm1 + q0,
+// s_2 = qm1 - 2q0 + qp1, s_3 = q0 - 2qp1 + qp2 and r_1 = qm2 - 4qm1 + 3q0,
+// r_2 = qm1 - qp1, r_3 = 3q0 - 4qp1 + qp2: the same quantities the Jiang-Shu
+// smoothness indicators beta_k = 13/12 s_k^2 + 1/4 r_k^2 square
+// (reconstruction.f90:699-704).  With a_k = gamma_k i_k, i_k = 1/(eps + beta_k)^2,
+//   sum_k omega_k p_k(xi) = q0 + sum_k gamma_k (+-hx u_k + tau v_k) / sum_k gamma_k i_k,
+// u_k = i_k r_k, v_k = i_k s_k formed once per stencil: 10 packed operations per
+// point where the tabulated three-term candidates take 18.  (hx, tau) of a point are
+// read off the reference's tabulated candidate-2 coefficients c of qm1 and qp1:
+// hx = (c_qp1 - c_qm1)/2, tau = (c_qm1 + c_qp1)/2.  Z: q0 is an exact zero (values
+// taken as deviations from the stencil's own centre), whose terms are dropped.
+struct WenoUV2 {
+  f2 u1, u2, u3, v1, v2, v3, i1, i2, i3;
+};
 
-// reciprocals of the squared smoothness indicators (sum-of-squares form)
-__device__ __forceinline__ void weno_rd_x2(f2 qm2, f2 qm1, f2 q0, f2 qp1, f2 qp2, f2& i1, f2& i2,
-                                           f2& i3) {
+template <bool Z>
+__device__ __forceinline__ WenoUV2 weno_uv_x2(f2 qm2, f2 qm1, f2 q0, f2 qp1, f2 qp2) {
   const f2 m2 = f2_splat(-2.f), m4 = f2_splat(-4.f), c3 = f2_splat(3.f);
+  f2 s1, r1, s2, r2, s3, r3;
+  if constexpr (Z) {
+    s1 = fma2(m2, qm1, qm2);
+    r1 = fma2(m4, qm1, qm2);
+    s2 = add2(qm1, qp1);
+    s3 = fma2(m2, qp1, qp2);
+    r3 = fma2(m4, qp1, qp2);
+  } else {
+    s1 = add2(fma2(m2, qm1, qm2), q0);
+    r1 = fma2(c3, q0, fma2(m4, qm1, qm2));
+    s2 = add2(fma2(m2, q0, qm1), qp1);
+    s3 = add2(fma2(m2, qp1, q0), qp2);
+    r3 = fma2(c3, q0, fma2(m4, qp1, qp2));
+  }
+  r2 = sub2(qm1, qp1);
+  // eps + beta_k as a sum of squares: never below eps
   const f2 c13 = f2_splat(13.f / 12.f), c4 = f2_splat(0.25f), eps = f2_splat(kWenoEpsF);
-  const f2 s1 = add2(fma2(m2, qm1, qm2), q0), r1 = fma2(c3, q0, fma2(m4, qm1, qm2));
-  const f2 s2 = add2(fma2(m2, q0, qm1), qp1), r2 = sub2(qm1, qp1);
-  const f2 s3 = add2(fma2(m2, qp1, q0), qp2), r3 = fma2(c3, q0, fma2(m4, qp1, qp2));
-  const f2 t1 = add2(eps, fma2(mul2(c13, s1), s1, mul2(mul2(c4, r1), r1)));
-  const f2 t2 = add2(eps, fma2(mul2(c13, s2), s2, mul2(mul2(c4, r2), r2)));
-  const f2 t3 = add2(eps, fma2(mul2(c13, s3), s3, mul2(mul2(c4, r3), r3)));
-  i1 = rcp2(mul2(t1, t1));
-  i2 = rcp2(mul2(t2, t2));
-  i3 = rcp2(mul2(t3, t3));
+  const f2 t1 = fma2(mul2(c13, s1), s1, fma2(mul2(c4, r1), r1, eps));
+  const f2 t2 = fma2(mul2(c13, s2), s2, fma2(mul2(c4, r2), r2, eps));
+  const f2 t3 = fma2(mul2(c13, s3), s3, fma2(mul2(c4, r3), r3, eps));
+  WenoUV2 w;
+  w.i1 = rcp2(mul2(t1, t1));
+  w.i2 = rcp2(mul2(t2, t2));
+  w.i3 = rcp2(mul2(t3, t3));
+  w.u1 = mul2(w.i1, r1);
+  w.u2 = mul2(w.i2, r2);
+  w.u3 = mul2(w.i3, r3);
+  w.v1 = mul2(w.i1, s1);
+  w.v2 = mul2(w.i2, s2);
+  w.v3 = mul2(w.i3, s3);
+  return w;
 }
 
-__device__ __forceinline__ f2 weno_point_x2(float g1, float g2, float g3, f2 i1, f2 i2, f2 i3, f2 W1,
-                                            f2 W2, f2 W3) {
-  const f2 a1 = mul2(f2_splat(g1), i1), a2 = mul2(f2_splat(g2), i2), a3 = mul2(f2_splat(g3), i3);
-  const f2 num = fma2(a3, W3, fma2(a2, W2, mul2(a1, W1)));
-  return mul2(num, rcp2(add2(add2(a1, a2), a3)));
+// One reconstruction point: its linear weights gamma_k and (hx, tau), folded into
+// FP32 coefficients at compile time.
+struct WenoGp {
+  float cu1, cu2, cu3, cv1, cv2, cv3, g1, g2, g3;
+};
+__host__ __device__ constexpr WenoGp weno_gp(double g1, double g2, double g3, double hx, double tau) {
+  return {float(g1 * hx), float(-g2 * hx), float(-g3 * hx), float(g1 * tau), float(g2 * tau),
+          float(g3 * tau), float(g1),      float(g2),       float(g3)};
+}
+// hx and tau of a second-sweep Gauss node from the candidate-2 coefficients
+__host__ __device__ constexpr double gp_hx(double c_qm1, double c_qp1) { return 0.5 * (c_qp1 - c_qm1); }
+__host__ __device__ constexpr double gp_tau(double c_qm1, double c_qp1) { return 0.5 * (c_qm1 + c_qp1); }
+
+template <bool Z>
+__device__ __forceinline__ f2 weno_gp_x2(const WenoUV2& t, f2 q0, const WenoGp c) {
+  f2 num = mul2(f2_splat(c.cu1), t.u1);
+  num = fma2(f2_splat(c.cu2), t.u2, num);
+  num = fma2(f2_splat(c.cu3), t.u3, num);
+  num = fma2(f2_splat(c.cv1), t.v1, num);
+  num = fma2(f2_splat(c.cv2), t.v2, num);
+  num = fma2(f2_splat(c.cv3), t.v3, num);
+  const f2 den = fma2(f2_splat(c.g3), t.i3, fma2(f2_splat(c.g2), t.i2, mul2(f2_splat(c.g1), t.i1)));
+  const f2 rd = rcp2(den);
+  if constexpr (Z)
+    return mul2(num, rd);
+  else
+    return fma2(num, rd, q0);
 }
 
-// Two first sweeps (reconstruction.f90:673-755).
+// Two first sweeps (reconstruction.f90:673-755): the faces xi = -1/2 (hx = -1/4,
+// tau = 1/12, gamma = 3/10, 3/5, 1/10) and xi = +1/2 (mirrored).
+template <bool Z = false>
 __device__ __forceinline__ void weno5_first_x2(f2 qm2, f2 qm1, f2 q0, f2 qp1, f2 qp2, f2& wm,
                                                f2& wp) {
-  f2 i1, i2, i3;
-  weno_rd_x2(qm2, qm1, q0, qp1, qp2, i1, i2, i3);
-  const float s6 = 1.f / 6.f;
-  f2 W1 = lin3(-s6, qm2, 5.f * s6, qm1, 2.f * s6, q0);
-  f2 W2 = lin3(2.f * s6, qm1, 5.f * s6, q0, -s6, qp1);
-  f2 W3 = lin3(11.f * s6, q0, -7.f * s6, qp1, 2.f * s6, qp2);
-  wm = weno_point_x2(0.3f, 0.6f, 0.1f, i1, i2, i3, W1, W2, W3);
-  W1 = lin3(2.f * s6, qm2, -7.f * s6, qm1, 11.f * s6, q0);
-  W2 = lin3(-s6, qm1, 5.f * s6, q0, 2.f * s6, qp1);
-  W3 = lin3(2.f * s6, q0, 5.f * s6, qp1, -s6, qp2);
-  wp = weno_point_x2(0.1f, 0.6f, 0.3f, i1, i2, i3, W1, W2, W3);
+  const WenoUV2 t = weno_uv_x2<Z>(qm2, qm1, q0, qp1, qp2);
+  constexpr WenoGp cm = weno_gp(0.3, 0.6, 0.1, -0.25, 1.0 / 12.0);
+  constexpr WenoGp cp = weno_gp(0.1, 0.6, 0.3, 0.25, 1.0 / 12.0);
+  wm = weno_gp_x2<Z>(t, q0, cm);
+  wp = weno_gp_x2<Z>(t, q0, cp);
 }
 
-// Two second sweeps (reconstruction.f90:999-1136), the coefficients of weno5_second.
+// Two second sweeps (reconstruction.f90:999-1136): the 4 Gauss nodes with the
+// reference's tabulated linear weights; (hx, tau) from its candidate-2 rows.
+template <bool Z = false>
 __device__ __forceinline__ void weno5_second_x2(f2 qm2, f2 qm1, f2 q0, f2 qp1, f2 qp2, f2 w[4]) {
-  f2 i1, i2, i3;
-  weno_rd_x2(qm2, qm1, q0, qp1, qp2, i1, i2, i3);
-  f2 W1, W2, W3;
-  W1 = lin3(-0.1642562761719537f, qm2, 0.7590807081409336f, qm1, 0.4051755680310201f, q0);
-  W2 = lin3(0.2663118796250726f, qm1, 0.8979443965468811f, q0, -0.1642562761719537f, qp1);
-  W3 = lin3(1.6968800354220990f, q0, -0.9631919150471715f, qp1, 0.2663118796250726f, qp2);
-  w[0] = weno_point_x2(0.2658420974778319f, 0.6112504900322486f, 0.1229074124899195f, i1, i2, i3,
-                       W1, W2, W3);
-  W1 = lin3(-0.1122135388132497f, qm2, 0.3944175994189276f, qm1, 0.7177959393943222f, q0);
-  W2 = lin3(0.0577769829791784f, qm1, 1.0544365558340714f, q0, -0.1122135388132497f, qp1);
-  W3 = lin3(1.2277675047716066f, q0, -0.2855444877507849f, qp1, 0.0577769829791784f, qp2);
-  w[1] = weno_point_x2(0.1281641584355059f, 0.5219691498503563f, 0.3498666917141379f, i1, i2, i3,
-                       W1, W2, W3);
-  W1 = lin3(0.0577769829791784f, qm2, -0.2855444877507849f, qm1, 1.2277675047716066f, q0);
-  W2 = lin3(-0.1122135388132497f, qm1, 1.0544365558340714f, q0, 0.0577769829791784f, qp1);
-  W3 = lin3(0.7177959393943222f, q0, 0.3944175994189276f, qp1, -0.1122135388132497f, qp2);
-  w[2] = weno_point_x2(0.3498666917141379f, 0.5219691498503563f, 0.1281641584355059f, i1, i2, i3,
-                       W1, W2, W3);
-  W1 = lin3(0.2663118796250726f, qm2, -0.9631919150471715f, qm1, 1.6968800354220990f, q0);
-  W2 = lin3(-0.1642562761719537f, qm1, 0.8979443965468811f, q0, 0.2663118796250726f, qp1);
-  W3 = lin3(0.4051755680310201f, q0, 0.7590807081409336f, qp1, -0.1642562761719537f, qp2);
-  w[3] = weno_point_x2(0.1229074124899195f, 0.6112504900322486f, 0.2658420974778319f, i1, i2, i3,
-                       W1, W2, W3);
+  const WenoUV2 t = weno_uv_x2<Z>(qm2, qm1, q0, qp1, qp2);
+  constexpr double a0 = 0.2663118796250726, b0 = -0.1642562761719537;  // node 0: c_qm1, c_qp1
+  constexpr double a1 = 0.0577769829791784, b1 = -0.1122135388132497;  // node 1
+  constexpr WenoGp c0 = weno_gp(0.2658420974778319, 0.6112504900322486, 0.1229074124899195,
+                                gp_hx(a0, b0), gp_tau(a0, b0));
+  constexpr WenoGp c1 = weno_gp(0.1281641584355059, 0.5219691498503563, 0.3498666917141379,
+                                gp_hx(a1, b1), gp_tau(a1, b1));
+  constexpr WenoGp c2 = weno_gp(0.3498666917141379, 0.5219691498503563, 0.1281641584355059,
+                                gp_hx(b1, a1), gp_tau(b1, a1));
+  constexpr WenoGp c3 = weno_gp(0.1229074124899195, 0.6112504900322486, 0.2658420974778319,
+                                gp_hx(b0, a0), gp_tau(b0, a0));
+  w[0] = weno_gp_x2<Z>(t, q0, c0);
+  w[1] = weno_gp_x2<Z>(t, q0, c1);
+  w[2] = weno_gp_x2<Z>(t, q0, c2);
+  w[3] = weno_gp_x2<Z>(t, q0, c3);
 }
 
 // ConsToPrim (equation.f90:912-945): u = hu / (h + MIN_DEPTH / h).  EXACT rounds

@@ -225,10 +225,12 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const i
       // U(1) = V(1) = h; rows (j0+rr)-2..+2 -> tile rows rr+1..rr+5; col i0-2+cc -> cc+1
       f2 q[5], w[4];
 #pragma unroll
-      for (int k = 0; k < 5; ++k)
-        q[k] = f2_pack(dev(0, rr + 1 + k, cc + 1, rr + 3, cc + 1),
-                       dev(0, rr + 2 + k, cc + 1, rr + 4, cc + 1));
-      weno5_second_x2(q[0], q[1], q[2], q[3], q[4], w);
+      for (int k = 0; k < 5; ++k)  // k = 2 is each stencil's centre: an exact zero
+        if (k != 2)
+          q[k] = f2_pack(dev(0, rr + 1 + k, cc + 1, rr + 3, cc + 1),
+                         dev(0, rr + 2 + k, cc + 1, rr + 4, cc + 1));
+      q[2] = f2_splat(0.f);
+      weno5_second_x2<true>(q[0], q[1], q[2], q[3], q[4], w);
 #pragma unroll
       for (int g = 0; g < 4; ++g)
         f2_unpack(w[g], sVt[(g * TY + rr) * SW_ + cc], sVt[(g * TY + rr + 1) * SW_ + cc]);
@@ -250,10 +252,13 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const i
         const int rr = 2 * rp;
         f2 q[5];
 #pragma unroll
-        for (int k = 0; k < 5; ++k)
-          q[k] = f2_pack(dev(v, rr + 1, cc + k, rr + 1, cc + 2), dev(v, rr + 2, cc + k, rr + 2, cc + 2));
+        for (int k = 0; k < 5; ++k)  // k = 2 is each stencil's centre: an exact zero
+          if (k != 2)
+            q[k] = f2_pack(dev(v, rr + 1, cc + k, rr + 1, cc + 2),
+                           dev(v, rr + 2, cc + k, rr + 2, cc + 2));
+        q[2] = f2_splat(0.f);
         f2 wm, wp;
-        weno5_first_x2(q[0], q[1], q[2], q[3], q[4], wm, wp);
+        weno5_first_x2<true>(q[0], q[1], q[2], q[3], q[4], wm, wp);
         f2_unpack(wm, sTM[(v * FH + rr) * FW + cc], sTM[(v * FH + rr + 1) * FW + cc]);
         f2_unpack(wp, sTP[(v * FH + rr) * FW + cc], sTP[(v * FH + rr + 1) * FW + cc]);
       }
@@ -354,10 +359,13 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const i
         // V rows (j0-1+rr)-2 .. +2 -> tile rows rr..rr+4; col (i0-2+cc) -> tile col cc+1
         f2 q[5];
 #pragma unroll
-        for (int k = 0; k < 5; ++k)
-          q[k] = f2_pack(dev(v, rr + k, cc + 1, rr + 2, cc + 1), dev(v, rr + k + 1, cc + 1, rr + 3, cc + 1));
+        for (int k = 0; k < 5; ++k)  // k = 2 is each stencil's centre: an exact zero
+          if (k != 2)
+            q[k] = f2_pack(dev(v, rr + k, cc + 1, rr + 2, cc + 1),
+                           dev(v, rr + k + 1, cc + 1, rr + 3, cc + 1));
+        q[2] = f2_splat(0.f);
         f2 wm, wp;
-        weno5_first_x2(q[0], q[1], q[2], q[3], q[4], wm, wp);
+        weno5_first_x2<true>(q[0], q[1], q[2], q[3], q[4], wm, wp);
         f2_unpack(wm, sTM[(v * FH + rr) * FW + cc], sTM[(v * FH + rr + 1) * FW + cc]);
         f2_unpack(wp, sTP[(v * FH + rr) * FW + cc], sTP[(v * FH + rr + 1) * FW + cc]);
       }
