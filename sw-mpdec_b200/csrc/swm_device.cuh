@@ -496,11 +496,14 @@ __device__ __forceinline__ void limit_h(const Grid& gr, double Vc, double wm[4],
     double mmin = csi;
     if (wm[g] < mmin) mmin = wm[g];
     if (wp[g] < mmin) mmin = wp[g];
+    // theta = min(1, |a/m|) is exactly 1 when |a| >= |m|: the quotient is then >= 1,
+    // and rounding keeps it there; the division only runs when it can limit
+    const double ta = Vc - kMinDepth, tm = Vc - mmin;
     double theta;
-    if (Vc == mmin)
+    if (Vc == mmin || fabs(ta) >= fabs(tm))
       theta = 1.;
     else
-      theta = dmin(1., fabs((Vc - kMinDepth) / (Vc - mmin)));
+      theta = dmin(1., fabs(ta / tm));
     wp[g] = Vc + theta * (wp[g] - Vc);
     wm[g] = Vc + theta * (wm[g] - Vc);
   }
@@ -524,11 +527,12 @@ __device__ __forceinline__ void limit_h_dev(const Grid& gr, double Vc, const flo
     double mmin = csi;
     if ((double)dm[g] < mmin) mmin = (double)dm[g];
     if ((double)dp[g] < mmin) mmin = (double)dp[g];
+    const double ta = Vc - kMinDepth;
     double theta;
-    if (mmin == 0.)
+    if (mmin == 0. || fabs(ta) >= fabs(mmin))  // the quotient would be >= 1
       theta = 1.;
     else
-      theta = dmin(1., fabs((Vc - kMinDepth) / mmin));
+      theta = dmin(1., fabs(ta / mmin));
     wp[g] = Vc + theta * (double)dp[g];
     wm[g] = Vc + theta * (double)dm[g];
   }
