@@ -70,7 +70,7 @@ struct RhsSmem {
   static constexpr int nW = 2 * 3 * 4 * (WX > WY ? WX : WY);      // double
   static constexpr int nFX = 3 * TY * (TX + 1);                   // double
   static constexpr int nFY = 3 * (TY + 1) * TX;                   // double
-  // split form: V also as float pairs hi + lo (hi = fl32(V), lo = fl32(V - hi))
+  // split form: V also as interleaved FP32 (hi, lo) pairs (hi = fl32(V), lo = fl32(V - hi))
   static constexpr int nVF = std::is_same<T, float>::value ? 2 * nV : 0;  // float
   // split form: the source term's y sweeps [4][TY][TX+4] in a buffer of their own, so
   // they can run in the x second-sweep phase (the FP64 form reuses the first-sweep area)
@@ -137,6 +137,16 @@ __device__ __forceinline__ void face_pass(const Grid& gr, Flux&& flux, Store&& s
   }
 }
 
+// Split form: the first sweeps of two rows (wm, wp packed by row) stored as the (m, p)
+// pairs of row 0 at p[0] and of row 1 at p[pitch].
+__device__ __forceinline__ void store_mp(unsigned long long* p, int pitch, f2 wm, f2 wp) {
+  float m0, m1, p0, p1;
+  f2_unpack(wm, m0, m1);
+  f2_unpack(wp, p0, p1);
+  p[0] = f2_pack(m0, p0).v;
+  p[pitch] = f2_pack(m1, p1).v;
+}
+
 // MODE: 0 FP64 (EXACT per translation unit), 1 SPLIT.  One CTA, tile origin (i0, j0).
 template <int MODE>
 __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const int j0) {
@@ -151,8 +161,8 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const i
   double* sFX = sW + SM::nW;                         // [3][TY][TX+1]
   double* sFY = sFX + SM::nFX;                       // [3][TY+1][TX]
   T* sF1 = reinterpret_cast<T*>(sFY + SM::nFY);      // [2][3][...]
-  float* sVh = reinterpret_cast<float*>(sF1 + SM::nF1);  // split: [3][VY][VX] hi parts
-  float* sVl = sVh + SM::nV;                              //        and lo parts
+  // split: [3][VY][VX] (hi, lo) pairs, one 8-byte load each
+  unsigned long long* sVhl = reinterpret_cast<unsigned long long*>(sF1 + SM::nF1);
 
   const Grid& gr = a.gr;
   const int nx = gr.nx, ny = gr.ny;
@@ -197,8 +207,7 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const i
 #pragma unroll
       for (int w = 0; w < 3; ++w) {
         const float hi = (float)qv[w];
-        sVh[(w * VY + cy) * VX + cx] = hi;
-        sVl[(w * VY + cy) * VX + cx] = (float)(qv[w] - (double)hi);
+        sVhl[(w * VY + cy) * VX + cx] = f2_pack(hi, (float)(qv[w] - (double)hi)).v;
       }
     }
   }
@@ -209,13 +218,15 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const i
   // one FP32 rounding, the same accuracy as rounding the FP64 difference
   auto dev = [&](int v, int y, int x, int yc, int xc) -> float {
     const int k = (v * VY + y) * VX + x, kc = (v * VY + yc) * VX + xc;
-    return (sVh[k] - sVh[kc]) + (sVl[k] - sVl[kc]);
+    float dh, dl;
+    f2_unpack(sub2(f2{sVhl[k]}, f2{sVhl[kc]}), dh, dl);
+    return dh + dl;
   };
 
   // source term's y sweeps of h at the 4 y Gauss points (split form: own buffer)
   const bool has_src = gr.bathy > 0;
   constexpr int SW_ = TX + 4;  // y-sweep columns i0-2..i0+TX+1
-  T* sVt = (MODE == 1) ? reinterpret_cast<T*>(sVl + SM::nV) : sF1;  // [4][TY][TX+4]
+  T* sVt = (MODE == 1) ? reinterpret_cast<T*>(sVhl + SM::nV) : sF1;  // [4][TY][TX+4]
   auto src_sweeps_split = [&]() {
     if constexpr (MODE == 1) {
     static_assert(TY % 2 == 0, "row pairs");
@@ -243,6 +254,7 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const i
     constexpr int FW = TX + 2, FH = TY + 4;  // first sweeps: cols i0-1..i0+TX, rows j0-2..j0+TY+1
     T* sTM = sF1;
     T* sTP = sF1 + 3 * FH * FW;
+    unsigned long long* sTMP = reinterpret_cast<unsigned long long*>(sF1);  // split: (m, p) pairs
     if constexpr (MODE == 1) {
       // two rows per item (packed pairs), deviations from each stencil's centre
       static_assert(FH % 2 == 0, "row pairs");
@@ -259,8 +271,7 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const i
         q[2] = f2_splat(0.f);
         f2 wm, wp;
         weno5_first_x2<true>(q[0], q[1], q[2], q[3], q[4], wm, wp);
-        f2_unpack(wm, sTM[(v * FH + rr) * FW + cc], sTM[(v * FH + rr + 1) * FW + cc]);
-        f2_unpack(wp, sTP[(v * FH + rr) * FW + cc], sTP[(v * FH + rr + 1) * FW + cc]);
+        store_mp(sTMP + (v * FH + rr) * FW + cc, FW, wm, wp);
       }
     } else {
       for (int it = tid; it < 3 * FH * FW; it += NT) {
@@ -284,9 +295,8 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const i
         f2 q[5], w[4];
 #pragma unroll
         for (int k = 0; k < 5; ++k) {
-          T base = dev(v, rr + 1 + k, cc + 2, rr + 3, cc + 2);  // row offset to the centre row
-          q[k] = f2_pack(base + sTM[(v * FH + rr + k) * FW + cc],
-                         base + sTP[(v * FH + rr + k) * FW + cc]);
+          const float base = dev(v, rr + 1 + k, cc + 2, rr + 3, cc + 2);  // row offset to the centre row
+          q[k] = add2(f2_splat(base), f2{sTMP[(v * FH + rr + k) * FW + cc]});
         }
         weno5_second_x2(q[0], q[1], q[2], q[3], q[4], w);
 #pragma unroll
@@ -349,6 +359,7 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const i
     constexpr int FW = TX + 4, FH = TY + 2;  // first sweeps: cols i0-2..i0+TX+1, rows j0-1..j0+TY
     T* sTM = sF1;
     T* sTP = sF1 + 3 * FH * FW;
+    unsigned long long* sTMP = reinterpret_cast<unsigned long long*>(sF1);  // split: (m, p) pairs
     if constexpr (MODE == 1) {
       // two rows per item (packed pairs): the vertical stencils of rows rr and rr+1
       // share four of their six values
@@ -366,8 +377,7 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const i
         q[2] = f2_splat(0.f);
         f2 wm, wp;
         weno5_first_x2<true>(q[0], q[1], q[2], q[3], q[4], wm, wp);
-        f2_unpack(wm, sTM[(v * FH + rr) * FW + cc], sTM[(v * FH + rr + 1) * FW + cc]);
-        f2_unpack(wp, sTP[(v * FH + rr) * FW + cc], sTP[(v * FH + rr + 1) * FW + cc]);
+        store_mp(sTMP + (v * FH + rr) * FW + cc, FW, wm, wp);
       }
     } else {
       for (int it = NT - 1 - tid; it < 3 * FH * FW; it += NT) {  // reversed: balances the x faces
@@ -394,9 +404,8 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const i
         f2 q[5], w[4];
 #pragma unroll
         for (int k = 0; k < 5; ++k) {
-          T base = dev(v, rr + 2, cc + 1 + k, rr + 2, cc + 3);
-          q[k] = f2_pack(base + sTM[(v * FH + rr) * FW + cc + k],
-                         base + sTP[(v * FH + rr) * FW + cc + k]);
+          const float base = dev(v, rr + 2, cc + 1 + k, rr + 2, cc + 3);
+          q[k] = add2(f2_splat(base), f2{sTMP[(v * FH + rr) * FW + cc + k]});
         }
         weno5_second_x2(q[0], q[1], q[2], q[3], q[4], w);
 #pragma unroll
