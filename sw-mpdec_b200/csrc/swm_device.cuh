@@ -63,6 +63,14 @@ __device__ __forceinline__ float rcp_(float x) {
   return r;
 }
 
+// FP32 square root by the hardware approximation (relative error ~2^-23); for the
+// split form's wave-speed bound, which only scales the Rusanov jump term.
+__device__ __forceinline__ float sqrt_approx(float x) {
+  float r;
+  asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
 // Correctly rounded x / y from a shared correctly rounded reciprocal r = RN(1/y):
 // two residual corrections with FMA (Markstein, IBM J. Res. Dev. 34(1), 1990;
 // Theorem 8.10 of Muller et al., Handbook of Floating-Point Arithmetic): with r
@@ -470,7 +478,8 @@ __device__ __forceinline__ void rusanov(double g, double hL, double nL, double t
   double FR2 = hR * nR * tR;
   double lam;
   if (LAM32) {
-    float fl = (float)nL + sqrtf((float)(g * hL)), fr = (float)nR + sqrtf((float)(g * hR));
+    float fl = (float)nL + sqrt_approx((float)(g * hL)),
+          fr = (float)nR + sqrt_approx((float)(g * hR));
     lam = (double)fmaxf(fabsf(fl), fabsf(fr));
   } else {
     double fastL = nL + sqrt(g * hL), fastR = nR + sqrt(g * hR);

@@ -518,22 +518,31 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const i
       if (!EX && a.src_col) {
         // separable gradient: S_hu = -g sum_a Pw_a sum_b Qw_b h_ab,
         //                     S_hv = -g sum_b Tw_b sum_a Rw_a h_ab
-        const double* pc = a.src_col + 8 * (size_t)gi;
-        const double* pr = a.src_row + 8 * (size_t)gj;
+        // 16-byte loads of the factor rows (64 bytes per column / row, 16-byte aligned)
+        double pc[8], pr[8];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const double2 c2 = __ldg(reinterpret_cast<const double2*>(a.src_col + 8 * (size_t)gi) + q);
+          const double2 r2 = __ldg(reinterpret_cast<const double2*>(a.src_row + 8 * (size_t)gj) + q);
+          pc[2 * q] = c2.x;
+          pc[2 * q + 1] = c2.y;
+          pr[2 * q] = r2.x;
+          pr[2 * q + 1] = r2.y;
+        }
         double s1 = 0.0, s2 = 0.0;
 #pragma unroll
         for (int aa = 0; aa < 4; ++aa) {
           double in = 0.0;
 #pragma unroll
-          for (int b = 0; b < 4; ++b) in = fma(__ldg(pr + b), hq[aa][b], in);
-          s1 = fma(__ldg(pc + aa), in, s1);
+          for (int b = 0; b < 4; ++b) in = fma(pr[b], hq[aa][b], in);
+          s1 = fma(pc[aa], in, s1);
         }
 #pragma unroll
         for (int b = 0; b < 4; ++b) {
           double in = 0.0;
 #pragma unroll
-          for (int aa = 0; aa < 4; ++aa) in = fma(__ldg(pc + 4 + aa), hq[aa][b], in);
-          s2 = fma(__ldg(pr + 4 + b), in, s2);
+          for (int aa = 0; aa < 4; ++aa) in = fma(pc[4 + aa], hq[aa][b], in);
+          s2 = fma(pr[4 + b], in, s2);
         }
         S1 = -gr.g * s1;
         S2 = -gr.g * s2;
