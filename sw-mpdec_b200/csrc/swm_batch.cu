@@ -62,6 +62,7 @@ struct BProblem {
   double *cS = nullptr, *cW = nullptr, *cE = nullptr, *cN = nullptr, *cD = nullptr;
   double *xa = nullptr, *xb = nullptr;
   double *src_col = nullptr, *src_row = nullptr, *bgrad = nullptr;
+  SrcSplit *src_cols = nullptr, *src_rows = nullptr;
   double* save[3] = {};  // state copy used while tuning
 };
 
@@ -167,6 +168,12 @@ static int batch_alloc_problem(swm_batch* b, BProblem& q) {
       return rc;
     BCK(cudaMemcpy(q.src_col, col.data(), sizeof(double) * col.size(), cudaMemcpyHostToDevice));
     BCK(cudaMemcpy(q.src_row, row.data(), sizeof(double) * row.size(), cudaMemcpyHostToDevice));
+    std::vector<SrcSplit> cols, rows;
+    host_source_split(col, row, cols, rows);
+    if ((rc = b->alloc(&q.src_cols, cols.size())) || (rc = b->alloc(&q.src_rows, rows.size())))
+      return rc;
+    BCK(cudaMemcpy(q.src_cols, cols.data(), sizeof(SrcSplit) * cols.size(), cudaMemcpyHostToDevice));
+    BCK(cudaMemcpy(q.src_rows, rows.data(), sizeof(SrcSplit) * rows.size(), cudaMemcpyHostToDevice));
   } else if (full_source_table(q.p)) {
     std::vector<double> tab;
     host_bgrad_table(q.p, gr, tab);
@@ -190,6 +197,8 @@ static RhsArgs batch_rhs_desc(const BProblem& q, const double* h, const double* 
   a.fym = q.fym[slot];
   a.src_col = q.src_col;
   a.src_row = q.src_row;
+  a.src_cols = q.src_cols;
+  a.src_rows = q.src_rows;
   a.bgrad = q.bgrad;
   return a;
 }

@@ -86,6 +86,7 @@ struct swm_solver {
   // bathymetry source tables: separable factors [nx][2][4], [ny][2][4] or the full
   // gradient [4][4][2][N] at the interior Gauss points
   double *src_col = nullptr, *src_row = nullptr;
+  SrcSplit *src_cols = nullptr, *src_rows = nullptr;
   double* bgrad = nullptr;
   // scalars
   double* dt_dev = nullptr;
@@ -185,6 +186,8 @@ static RhsArgs make_rhs_args(swm_solver* s, const double* h, const double* hu, c
   }
   a.src_col = s->src_col;
   a.src_row = s->src_row;
+  a.src_cols = s->src_cols;
+  a.src_rows = s->src_rows;
   a.bgrad = s->bgrad;
   return a;
 }
@@ -694,10 +697,19 @@ int swm_create(const swm_params* p, swm_handle* out) {
     int rc2 = s->dalloc(&s->src_col, col.size());
     if (!rc2) rc2 = s->dalloc(&s->src_row, row.size());
     if (rc2) return cleanup(rc2);
+    std::vector<SrcSplit> cols, rows;
+    host_source_split(col, row, cols, rows);
+    if (!rc2) rc2 = s->dalloc(&s->src_cols, cols.size());
+    if (!rc2) rc2 = s->dalloc(&s->src_rows, rows.size());
+    if (rc2) return cleanup(rc2);
     if (cudaMemcpy(s->src_col, col.data(), sizeof(double) * col.size(), cudaMemcpyHostToDevice) !=
             cudaSuccess ||
         cudaMemcpy(s->src_row, row.data(), sizeof(double) * row.size(), cudaMemcpyHostToDevice) !=
-            cudaSuccess)
+            cudaSuccess ||
+        cudaMemcpy(s->src_cols, cols.data(), sizeof(SrcSplit) * cols.size(),
+                   cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(s->src_rows, rows.data(), sizeof(SrcSplit) * rows.size(),
+                   cudaMemcpyHostToDevice) != cudaSuccess)
       return cleanup(fail(SWM_ERR_CUDA, "bathymetry factor upload failed"));
   } else if (full_source_table(*p)) {  // host libm (equation.f90:451-509)
     std::vector<double> tab;

@@ -8,6 +8,7 @@
 
 #include "../../include/swm.h"
 #include "swm_device.cuh"
+#include "swm_rhs.cuh"
 
 namespace swm {
 
@@ -153,6 +154,33 @@ inline void host_source_factors(const swm_params& p, const Grid& gr, std::vector
       row[8 * (size_t)j + q] = gr.qw[q] * Q;
       row[8 * (size_t)j + 4 + q] = gr.qw[q] * T;
     }
+}
+
+// The split form's records of the same factors (SrcSplit): FP32 factors, the column's
+// w R as (w R, w R) pairs, and the FP64 sums of each factor's four weights.
+inline void host_source_split(const std::vector<double>& col, const std::vector<double>& row,
+                              std::vector<SrcSplit>& cols, std::vector<SrcSplit>& rows) {
+  const size_t nx = col.size() / 8, ny = row.size() / 8;
+  cols.assign(nx, SrcSplit{});
+  rows.assign(ny, SrcSplit{});
+  for (size_t i = 0; i < nx; ++i) {
+    const double* c = &col[8 * i];
+    for (int q = 0; q < 4; ++q) {
+      cols[i].a[q] = (float)c[q];
+      cols[i].b[2 * q] = cols[i].b[2 * q + 1] = (float)c[4 + q];
+    }
+    cols[i].s[0] = ((c[0] + c[1]) + c[2]) + c[3];
+    cols[i].s[1] = ((c[4] + c[5]) + c[6]) + c[7];
+  }
+  for (size_t j = 0; j < ny; ++j) {
+    const double* r = &row[8 * j];
+    for (int q = 0; q < 4; ++q) {
+      rows[j].a[q] = (float)r[q];
+      rows[j].b[q] = (float)r[4 + q];
+    }
+    rows[j].s[0] = ((r[0] + r[1]) + r[2]) + r[3];
+    rows[j].s[1] = ((r[4] + r[5]) + r[6]) + r[7];
+  }
 }
 
 }  // namespace swm

@@ -24,6 +24,13 @@
 
 namespace swm {
 
+// Split-form bathymetry factor record (64 bytes, 16-byte aligned).
+struct SrcSplit {
+  float a[4];
+  float b[8];
+  double s[2];
+};
+
 struct RhsArgs {
   Grid gr;
   const double* h;
@@ -45,6 +52,11 @@ struct RhsArgs {
   // {w_b Q(y_b), w_b T(y_b)} for b_x = P Q, b_y = R T (split and FMA forms)
   const double* src_col;
   const double* src_row;
+  // nullable: the same factors for the split form as FP32 with their FP64 sums,
+  // one record per column (a = w P, b = (w R, w R) pairs, s = sum w P, sum w R) and per
+  // row (a = w Q, b = w T, s = sum w Q, sum w T)
+  const SrcSplit* src_cols;
+  const SrcSplit* src_rows;
   // nullable: b_x, b_y at the 16 interior Gauss points of every cell, evaluated on the
   // host with the analytic formula (equation.f90:451-509), planes [4][4][2][ny*nx]
   const double* bgrad;
@@ -484,26 +496,68 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const i
     double S1 = 0.0, S2 = 0.0;
     if (has_src) {
       double hq[4][4];  // [x-GP a][y-GP b]
+      bool done = false;
       if constexpr (MODE == 1) {
         const double hc = SV(0, rr + 3, cc + 3);
+        // depth deviations d_ab = h_ab - hc, y-GP rows b, b+1 packed: wb[b / 2][a]
+        f2 wb[2][4];
         T dv[5];
 #pragma unroll
-        for (int k = 0; k < 5; ++k) dv[k] = dev(0, rr + 3, cc + 1 + k, rr + 3, cc + 3);
+        for (int k = 0; k < 5; ++k)  // k = 2 is the centre: an exact zero
+          dv[k] = (k == 2) ? 0.f : dev(0, rr + 3, cc + 1 + k, rr + 3, cc + 3);
 #pragma unroll
-        for (int b = 0; b < 4; b += 2) {  // y-GP rows b, b+1 packed
+        for (int b = 0; b < 4; b += 2) {
           const T* r0 = &sVt[(b * TY + rr) * SW_ + cc];
           const T* r1 = &sVt[((b + 1) * TY + rr) * SW_ + cc];
-          f2 q[5], w[4];
+          f2 q[5];
 #pragma unroll
-          for (int k = 0; k < 5; ++k) q[k] = f2_pack(dv[k] + r0[k], dv[k] + r1[k]);
-          weno5_second_x2(q[0], q[1], q[2], q[3], q[4], w);
+          for (int k = 0; k < 5; ++k)
+            q[k] = (k == 2) ? f2_pack(r0[k], r1[k]) : f2_pack(dv[k] + r0[k], dv[k] + r1[k]);
+          weno5_second_x2(q[0], q[1], q[2], q[3], q[4], wb[b / 2]);
+        }
+        if (a.src_cols) {
+          // separable gradient on the deviations, the centre part in FP64:
+          //   S_hu = -g (hc sum_a Pw_a sum_b Qw_b + sum_a Pw_a sum_b Qw_b d_ab)
+          //   S_hv = -g (hc sum_a Rw_a sum_b Tw_b + sum_b Tw_b sum_a Rw_a d_ab)
+          const SrcSplit& C = a.src_cols[gi];
+          const SrcSplit& R = a.src_rows[gj];
+          const float4 P = __ldg(reinterpret_cast<const float4*>(C.a));
+          const ulonglong2 R01 = __ldg(reinterpret_cast<const ulonglong2*>(C.b));
+          const ulonglong2 R23 = __ldg(reinterpret_cast<const ulonglong2*>(C.b + 4));
+          const ulonglong2 Qp = __ldg(reinterpret_cast<const ulonglong2*>(R.a));
+          const ulonglong2 Tp = __ldg(reinterpret_cast<const ulonglong2*>(R.b));
+          const double2 cs = __ldg(reinterpret_cast<const double2*>(C.s));
+          const double2 rs = __ldg(reinterpret_cast<const double2*>(R.s));
+          const float Pa[4] = {P.x, P.y, P.z, P.w};
+          const f2 Ra[4] = {f2{R01.x}, f2{R01.y}, f2{R23.x}, f2{R23.y}};  // (R_a, R_a)
+          float s1d = 0.f;
 #pragma unroll
           for (int aa = 0; aa < 4; ++aa) {
-            float lo, hi;
-            f2_unpack(w[aa], lo, hi);
-            hq[aa][b] = hc + (double)lo;
-            hq[aa][b + 1] = hc + (double)hi;
+            float x, y;
+            f2_unpack(fma2(f2{Qp.y}, wb[1][aa], mul2(f2{Qp.x}, wb[0][aa])), x, y);
+            s1d = fmaf(Pa[aa], x + y, s1d);
           }
+          f2 r0 = mul2(Ra[0], wb[0][0]), r1 = mul2(Ra[0], wb[1][0]);
+#pragma unroll
+          for (int aa = 1; aa < 4; ++aa) {
+            r0 = fma2(Ra[aa], wb[0][aa], r0);
+            r1 = fma2(Ra[aa], wb[1][aa], r1);
+          }
+          float x, y;
+          f2_unpack(fma2(f2{Tp.y}, r1, mul2(f2{Tp.x}, r0)), x, y);
+          S1 = -gr.g * fma(hc, cs.x * rs.x, (double)s1d);
+          S2 = -gr.g * fma(hc, cs.y * rs.y, (double)(x + y));
+          done = true;
+        } else {
+#pragma unroll
+          for (int p = 0; p < 2; ++p)
+#pragma unroll
+            for (int aa = 0; aa < 4; ++aa) {
+              float lo, hi;
+              f2_unpack(wb[p][aa], lo, hi);
+              hq[aa][2 * p] = hc + (double)lo;
+              hq[aa][2 * p + 1] = hc + (double)hi;
+            }
         }
       } else {
 #pragma unroll
@@ -515,7 +569,8 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const i
           for (int aa = 0; aa < 4; ++aa) hq[aa][b] = (double)w[aa];
         }
       }
-      if (!EX && a.src_col) {
+      if (done) {
+      } else if (!EX && a.src_col) {
         // separable gradient: S_hu = -g sum_a Pw_a sum_b Qw_b h_ab,
         //                     S_hv = -g sum_b Tw_b sum_a Rw_a h_ab
         // 16-byte loads of the factor rows (64 bytes per column / row, 16-byte aligned)
