@@ -44,6 +44,7 @@ struct Grid {
   double qn[4];  // Gauss nodes on [-1/2, 1/2] (mesh.f90:128-129)
   double qw[4];  // Gauss weights (mesh.f90:127)
   double wgp[4][4];
+  float qwf[4];  // the Gauss weights rounded to FP32 (split-form limiter)
 };
 
 __device__ __forceinline__ int wrap(int i, int n) {
@@ -519,28 +520,25 @@ __device__ __forceinline__ void limit_h(const Grid& gr, double Vc, double wm[4],
 }
 
 // The same limiter on deviations d = W - Vc (split form): csi - Vc =
-// -(wL a' + wL b')/(1 - 2 wL) with a' = sum w_g dM_g, b' = sum w_g dP_g; theta is
-// formed in FP64 so that the limited depth V + theta*d stays >= MIN_DEPTH up to
-// FP64 rounding.
+// -(wL a' + wL b')/(1 - 2 wL) with a' = sum w_g dM_g, b' = sum w_g dP_g.  The sums,
+// csi and the minimum are FP32 (they only pick the deviation that binds); theta is
+// formed in FP64 from that deviation, so that the limited depth V + theta*d stays
+// >= MIN_DEPTH up to FP64 rounding for every face value d >= mmin.
 __device__ __forceinline__ void limit_h_dev(const Grid& gr, double Vc, const float dm[4],
                                             const float dp[4], double wm[4], double wp[4]) {
-  double alpha = 0., beta = 0.;
+  float alpha = 0.f, beta = 0.f;
 #pragma unroll
   for (int g = 0; g < 4; ++g) {
-    alpha = alpha + gr.qw[g] * (double)dm[g];
-    beta = beta + gr.qw[g] * (double)dp[g];
+    alpha = fmaf(gr.qwf[g], dm[g], alpha);
+    beta = fmaf(gr.qwf[g], dp[g], beta);
   }
-  double csi = -(kWLobatto * alpha + kWLobatto * beta) * kCsiRcp;
+  const float csi = -((float)kWLobatto * alpha + (float)kWLobatto * beta) * (float)kCsiRcp;
+  const double ta = Vc - kMinDepth;
 #pragma unroll
   for (int g = 0; g < 4; ++g) {
-    double mmin = csi;
-    if ((double)dm[g] < mmin) mmin = (double)dm[g];
-    if ((double)dp[g] < mmin) mmin = (double)dp[g];
-    const double ta = Vc - kMinDepth;
-    double theta;
-    if (mmin == 0. || fabs(ta) >= fabs(mmin))  // the quotient would be >= 1
-      theta = 1.;
-    else
+    const double mmin = (double)fminf(csi, fminf(dm[g], dp[g]));
+    double theta = 1.;
+    if (mmin != 0. && fabs(ta) < fabs(mmin))  // else the quotient would be >= 1
       theta = dmin(1., fabs(ta / mmin));
     wp[g] = Vc + theta * (double)dp[g];
     wm[g] = Vc + theta * (double)dm[g];

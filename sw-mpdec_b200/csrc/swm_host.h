@@ -41,6 +41,7 @@ inline Grid host_grid(const swm_params& p) {
   host_quadrature(gr.qn, gr.qw);
   for (int a = 0; a < 4; ++a)
     for (int b = 0; b < 4; ++b) gr.wgp[a][b] = gr.qw[a] * gr.qw[b];
+  for (int q = 0; q < 4; ++q) gr.qwf[q] = (float)gr.qw[q];
   return gr;
 }
 
