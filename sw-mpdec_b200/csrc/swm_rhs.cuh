@@ -306,9 +306,9 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const i
         float dm[4], dp[4];
         f2 q[5], w[4];
 #pragma unroll
-        for (int k = 0; k < 5; ++k) {
-          const float base = dev(v, rr + 1 + k, cc + 2, rr + 3, cc + 2);  // row offset to the centre row
-          q[k] = add2(f2_splat(base), f2{sTMP[(v * FH + rr + k) * FW + cc]});
+        for (int k = 0; k < 5; ++k) {  // k = 2 is the centre row: no offset
+          const f2 t = f2{sTMP[(v * FH + rr + k) * FW + cc]};
+          q[k] = (k == 2) ? t : add2(f2_splat(dev(v, rr + 1 + k, cc + 2, rr + 3, cc + 2)), t);
         }
         weno5_second_x2(q[0], q[1], q[2], q[3], q[4], w);
 #pragma unroll
@@ -415,9 +415,9 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const i
         float dm[4], dp[4];
         f2 q[5], w[4];
 #pragma unroll
-        for (int k = 0; k < 5; ++k) {
-          const float base = dev(v, rr + 2, cc + 1 + k, rr + 2, cc + 3);
-          q[k] = add2(f2_splat(base), f2{sTMP[(v * FH + rr) * FW + cc + k]});
+        for (int k = 0; k < 5; ++k) {  // k = 2 is the centre column: no offset
+          const f2 t = f2{sTMP[(v * FH + rr) * FW + cc + k]};
+          q[k] = (k == 2) ? t : add2(f2_splat(dev(v, rr + 2, cc + 1 + k, rr + 2, cc + 3)), t);
         }
         weno5_second_x2(q[0], q[1], q[2], q[3], q[4], w);
 #pragma unroll
