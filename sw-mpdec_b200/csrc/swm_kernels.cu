@@ -240,6 +240,20 @@ cudaError_t launch_summary(const double* h, int n, double* out, cudaStream_t s) 
 // den(h) = h^2 + max(h^2, MIN_DEPTH) (timediscretization.f90:913-924).
 __device__ __forceinline__ double patankar_den(double h) { return h * h + dmax(h * h, kMinDepth); }
 
+// 1/x for the fast forms' Patankar denominators (>= MIN_DEPTH) and diagonals (>= 1):
+// the FP32 hardware reciprocal of fl32(x) (relative error < 2^-22 against 1/x) refined
+// by two Newton-Raphson steps in FP64, e <- 1 - x r, r <- r + r e, which square the
+// error (2^-44, then below the final rounding).  The weights of a cell are the same
+// function of its depth wherever they are formed, so production and destruction
+// still cancel exactly.
+__device__ __forceinline__ double rcp_fast(double x) {
+  double r = (double)rcp_((float)x);
+  double e = fma(-x, r, 1.0);
+  r = fma(r, e, r);
+  e = fma(-x, r, 1.0);
+  return fma(r, e, r);
+}
+
 __device__ __forceinline__ double hp_read(const AssembleArgs& a, int m, int i, int j) {
   // m, i, j 0-based
   if (a.msteps == 2 && a.compat2) {
@@ -328,12 +342,12 @@ __device__ __forceinline__ void assemble_stage(const AssembleArgs& a, bool csr, 
     }
     o.hu[k] = au;
     o.hv[k] = av;
-    const double wK = hK >= kMinDepth ? (2. * hK) * __drcp_rn(patankar_den(hK)) : 0.;
+    const double wK = hK >= kMinDepth ? (2. * hK) * rcp_fast(patankar_den(hK)) : 0.;
 #pragma unroll
     for (int nb = 0; nb < 4; ++nb) {
       const double ilen = (nb == 0 || nb == 3) ? a.inv_dy : a.inv_dx;
       const double h = hL[nb];
-      const double wL = h >= kMinDepth ? (2. * h) * __drcp_rn(patankar_den(h)) : 0.;
+      const double wL = h >= kMinDepth ? (2. * h) * rcp_fast(patankar_den(h)) : 0.;
       const double aL = ilen * wL, aK = ilen * wK;
 #pragma unroll
       for (int r = 0; r < MS; ++r) {
@@ -401,7 +415,7 @@ __device__ __forceinline__ void assemble_stage(const AssembleArgs& a, bool csr, 
   } else if constexpr (FAST) {
     // the fast stencil solver iterates x = b/D - sum (M/D) x: the row divided by its
     // Diagonal, the rhs b = hp(1,.) (timediscretization.f90:887) in the D plane
-    const double rD = __drcp_rn(D);
+    const double rD = rcp_fast(D);
     o.cS[k] = M[0] * rD;
     o.cW[k] = M[1] * rD;
     o.cE[k] = M[2] * rD;

@@ -86,6 +86,33 @@ def test_rhs_forms_close(gpu, precision, tol, name, n):
     assert np.abs(got["Ut"] - ref["Ut"]).max() <= 4 * tol * f_scale / dx
 
 
+# The reference's other bathymetries (equation.f90:430-438) with their reference
+# initial states: the sin/cos bottom (separable: the split and FMA forms take the
+# per-column/row factors) and the bump (the full gradient table in every form).
+@pytest.mark.parametrize("bathy,ic,dom", [(1, 2, ((0.0, 0.0), (1.0, 1.0))),
+                                          (2, 6, ((-3.0, -1.5), (3.0, 2.5)))])
+@pytest.mark.parametrize("precision,tol", [("fp64", 0.0), ("fp64_fma", 5e-7), ("split", 2e-6)])
+def test_rhs_other_bathymetries(gpu, bathy, ic, dom, precision, tol):
+    nx, ny = 40, 36
+    o = O.Oracle(O.make_params(nx, ny, dom[0], dom[1], g=9.81, cfl=0.4, bathy_flag=bathy))
+    o.fill_ic(ic)
+    s = gpu.Solver(nx=nx, ny=ny, x0=dom[0], x1=dom[1], g=9.81, cfl=0.4, bathy_flag=bathy,
+                   bathy_par=(0.0,) * 5, precision=precision, solver="stencil", jacobi_block=4)
+    ref = o.rhs()
+    got = s.debug_rhs(o.get_state()[0])
+    if tol == 0.0:
+        for key in ("FX", "FY", "S", "Ut"):
+            assert np.array_equal(got[key], ref[key]), key
+        return
+    f_scale = max(np.abs(ref["FX"]).max(), np.abs(ref["FY"]).max(), 1.0)
+    for key in ("FX", "FY"):
+        assert np.abs(got[key] - ref[key]).max() <= tol * f_scale, key
+    s_scale = max(np.abs(ref["S"]).max(), 1.0)
+    assert np.abs(got["S"] - ref["S"]).max() <= tol * s_scale
+    dx = (dom[1][0] - dom[0][0]) / nx
+    assert np.abs(got["Ut"] - ref["Ut"]).max() <= 4 * tol * f_scale / dx
+
+
 def test_timestep_bitwise(gpu):
     c, o, s = make_pair(gpu, "vortex", 50)
     assert s.timestep() == o.timestep()
