@@ -496,7 +496,7 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const i
     double S1 = 0.0, S2 = 0.0;
     if (has_src) {
       double hq[4][4];  // [x-GP a][y-GP b]
-      bool done = false;
+      bool done = false;  // split form: S1, S2 already formed from the factor records
       if constexpr (MODE == 1) {
         const double hc = SV(0, rr + 3, cc + 3);
         // depth deviations d_ab = h_ab - hc, y-GP rows b, b+1 packed: wb[b / 2][a]
@@ -569,8 +569,7 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const i
           for (int aa = 0; aa < 4; ++aa) hq[aa][b] = (double)w[aa];
         }
       }
-      if (done) {
-      } else if (!EX && a.src_col) {
+      if (!done && !EX && a.src_col) {
         // separable gradient: S_hu = -g sum_a Pw_a sum_b Qw_b h_ab,
         //                     S_hv = -g sum_b Tw_b sum_a Rw_a h_ab
         // 16-byte loads of the factor rows (64 bytes per column / row, 16-byte aligned)
@@ -601,7 +600,7 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const i
         }
         S1 = -gr.g * s1;
         S2 = -gr.g * s2;
-      } else {
+      } else if (!done) {
         // S = sum_{a (x-GP)} sum_{b (y-GP)} W(a,b) * SourceFunc (equation.f90:380-388,
         // :408-410), gradient from the host table [x-GP][y-GP][comp][cell]
         const size_t nc = (size_t)nx * ny, cell = (size_t)gj * nx + gi;
