@@ -617,6 +617,12 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
   unsigned s = (unsigned)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
 }
+// 8-byte asynchronous global->shared copy through L1 (cp.async.ca), for arrays that
+// no CTA writes during the launch.
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem));
+}
 __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::);
 }
@@ -840,15 +846,18 @@ __device__ void stencil_tiles(const JacobiArgs& a, const double* xin, double* xo
           gi = small ? wrap(gi, nx) : wrap_near(gi, nx);
           const size_t g = row + gi;
           const int c = ly * HX + lx;
-          sS[c] = a.cS[g];
-          sW[c] = a.cW[g];
-          sE[c] = a.cE[g];
-          sN[c] = a.cN[g];
-          sD[c] = a.cD[g];
-          if (!RECIP || from_b) sB[c] = a.b[g];
+          // the system is read-only during the solve: 8-byte asynchronous copies;
+          // the iterate, which other CTAs wrote, by a load that bypasses L1
+          cp_async8(&sS[c], &a.cS[g]);
+          cp_async8(&sW[c], &a.cW[g]);
+          cp_async8(&sE[c], &a.cE[g]);
+          cp_async8(&sN[c], &a.cN[g]);
+          cp_async8(&sD[c], &a.cD[g]);
+          if (!RECIP || from_b) cp_async8(&sB[c], &a.b[g]);
           if (!from_b) x0[c] = __ldcg(&xin[g]);
         }
       }
+      cp_async_wait_all();
     }
     __syncthreads();
     if (first) {  // initial residual mean|0 - b| (jacobi_iteration.f90:69)
