@@ -289,8 +289,8 @@ __device__ __forceinline__ void weno5_second(T qm2, T qm1, T q0, T qp1, T qp2, T
 // ---------------------------------------------------------------------------------
 // Packed FP32 pairs for the split form: sm_100's f32x2 add/sub/mul/fma instructions
 // carry two independent reconstructions per issued instruction (the two faces of a
-// cell, or two neighbouring stencils).  The formulas are the non-EXACT ones above
-// with the 1/6 of the first sweep folded into its coefficients.
+// cell, or two neighbouring stencils).  The smoothness indicators are the non-EXACT
+// sums of squares above; the point values use the candidate-quadratic form below.
 struct f2 {
   unsigned long long v;
 };
