@@ -164,7 +164,9 @@ SWM_API int swm_timestep(swm_handle h, double *dt_min);
 
 /* One mPDeC5 (or mPDeC2) step of size dt from time t; the state is updated on
  * the device.  Replaces TimeDiscretizationByMPDeC5(t) (timediscretization.f90:458-566).
- * Returns SWM_WARN_JACOBI_MAXITER if a solve stopped at maxIter. */
+ * Returns SWM_WARN_JACOBI_MAXITER if a solve stopped at maxIter, and SWM_ERR_NAN if
+ * the new state holds a non-finite value or a negative depth: the step ends with
+ * TimeStep()'s reduction of the new state, which the next swm_timestep reuses. */
 SWM_API int swm_step(swm_handle h, double t, double dt);
 
 /* Steps from t to t_end with dt = min(TimeStep(), t_out - t, t_end - t), restating
@@ -201,6 +203,19 @@ SWM_API int swm_debug_rhs(swm_handle h, const double *U_ghosted, double *Ut, dou
 SWM_API int swm_debug_jacobi(swm_handle h, const double *mass, const double *diag, const double *rhs,
                      double *sol, int *iters);
 
+/* Failure paths a test can reach without a GPU fault.
+ * swm_debug_set_spin_limit: polls each grid-barrier wait of the handle's Jacobi
+ * launches makes before it gives up with SWM_ERR_WATCHDOG (default 2^26, about a
+ * second); limit <= 0 makes every wait that is not already open give up at once.
+ * The step's graph is rebuilt with the new limit.  Every step and debug solve
+ * starts from a cleared control block, so a handle stays usable after a watchdog.
+ * swm_debug_inject_alloc_failure: from now on the library's nth device or
+ * pinned-host allocation (process-wide, counted from this call) fails as if the
+ * allocator had; 0 disables.  *counted (nullable) receives the number of
+ * allocations made since the previous call. */
+SWM_API int swm_debug_set_spin_limit(swm_handle h, long long limit);
+SWM_API int swm_debug_inject_alloc_failure(long long nth, long long *counted);
+
 /* ---- allocation-free Jacobi solve ----
  * No counterpart in the reference (its jacobi() works on module arrays).  For
  * callers that cannot let a library allocate device memory -- drivers that own
@@ -209,16 +224,18 @@ SWM_API int swm_debug_jacobi(swm_handle h, const double *mass, const double *dia
  * cudaFree.  Solves one Patankar system (x <- (rhs - S x_S - W x_W - E x_E - N x_N)/D
  * on the periodic nx*ny grid, stop rule of jacobi_iteration.f90:52-87) with the
  * matrix-free stencil kernel, `block` sweeps per pass (1..8).  All arrays are the
- * caller's device memory, nx*ny doubles each, [ny][nx] row-major; rhs and sol
- * must not overlap.  Scratch is a static device array sized for at most
+ * caller's device memory, nx*ny doubles each, [ny][nx] row-major; sol is written
+ * while the others are read, so it must not overlap rhs or any coefficient plane
+ * (SWM_ERR_PARAM otherwise).  Scratch is a static device array sized for at most
  * 1,048,576 cells (8 MiB plus a small control block), held on every GPU that
  * loads the library until the process exits; larger grids are rejected with
  * SWM_ERR_PARAM.  The first call on each device looks up that array's device
  * address (cudaGetSymbolAddress) and the kernel's resident grid; make that first
  * call before any stream capture.  Every call shares the scratch: calls whose
  * work overlaps on the GPU (other streams, other host threads) race.  Runs on
- * `stream` (a cudaStream_t, 0 = legacy default) and returns after the solve with
- * the iteration count in *iters. */
+ * `stream` (a cudaStream_t, 0 = legacy default), then synchronises that stream to
+ * read the iteration count back, so a stream that is being captured is refused
+ * with SWM_ERR_STATE; returns after the solve with the count in *iters. */
 SWM_API int swm_jacobi_noalloc(int nx, int ny, const double *cS, const double *cW,
                                const double *cE, const double *cN, const double *cD,
                                const double *rhs, double *sol, int maxiter, double tol,

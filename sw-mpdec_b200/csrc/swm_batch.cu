@@ -303,7 +303,7 @@ static int batch_enqueue(swm_batch* b, int block) {
       ja.ctl = b->d_ctl;
       ja.iters = b->d_iters + (size_t)solve * b->n;
       ja.block = block;
-      ja.spin_limit = 1LL << 26;
+      ja.spin_limit = kDefaultSpinLimit;
       BCK(launch_jacobi_batch(ja, b->jac_blocks[block], b->fast, b->stream));
     }
     if (k < 5)

@@ -6,6 +6,7 @@
 // sequence of kernels below, captured once into a CUDA graph (dt is read from
 // device memory, so the graph is replayed unchanged every step).
 #include <array>
+#include <atomic>
 #include <cmath>
 #include <initializer_list>
 #include <utility>
@@ -28,6 +29,34 @@ thread_local std::string g_last_error;
 int fail(int code, const std::string& msg) {
   g_last_error = msg;
   return code;
+}
+
+// Host-side allocation-failure injection (swm_debug_inject_alloc_failure): the
+// library's device and pinned-host allocations are counted, and the one whose
+// number equals g_alloc_fail_at is refused as if the allocator had failed.
+std::atomic<long long> g_alloc_count{0};
+std::atomic<long long> g_alloc_fail_at{0};
+
+bool injected_alloc_failure() {
+  const long long n = ++g_alloc_count;
+  const long long at = g_alloc_fail_at.load();
+  return at > 0 && n == at;
+}
+
+cudaError_t lib_malloc(void** p, size_t bytes) {
+  if (injected_alloc_failure()) {
+    *p = nullptr;
+    return cudaErrorMemoryAllocation;
+  }
+  return cudaMalloc(p, bytes);
+}
+
+cudaError_t lib_malloc_host(void** p, size_t bytes) {
+  if (injected_alloc_failure()) {
+    *p = nullptr;
+    return cudaErrorMemoryAllocation;
+  }
+  return cudaMallocHost(p, bytes);
 }
 
 #define CK(call)                                                                         \
@@ -90,8 +119,8 @@ struct swm_solver {
   double* bgrad = nullptr;
   // scalars
   double* dt_dev = nullptr;
-  unsigned long long* lam = nullptr;
-  int* bad = nullptr;
+  unsigned long long* lam = nullptr;  // [2] LambdaMax bit patterns, then the flag
+  int* bad = nullptr;                 // inside the same allocation as lam
   JacobiCtl* ctl = nullptr;
   double* summary = nullptr;
   double* l1_scratch = nullptr;  // L1 error: 3 * kIcMaxBlocks partials + 3 results
@@ -108,13 +137,18 @@ struct swm_solver {
   // pinned host mirrors
   double* h_dt = nullptr;
   JacobiCtl* h_ctl = nullptr;
-  unsigned long long* h_lam = nullptr;
+  unsigned long long* h_lam = nullptr;  // pinned mirror of lam and bad (3 words)
   int* h_bad = nullptr;
   // graph
   cudaGraphExec_t graph = nullptr;
   bool graph_failed = false;
   int jac_blocks = 0;
   int n_solves = 0;
+  // grid-barrier watchdog of the Jacobi launches (polls before giving up)
+  long long spin_limit = kDefaultSpinLimit;
+  // the step's last launch computes LambdaMax and the non-finite/negative-depth flag
+  // of the new state; swm_timestep uses them while the state is unchanged
+  bool lam_fresh = false;
   // per-launch event profiling (swm_profile_step)
   bool profiling = false;
   std::vector<cudaEvent_t> prof_ev;
@@ -126,7 +160,7 @@ struct swm_solver {
   template <typename T>
   int dalloc(T** ptr, size_t count) {
     void* p_ = nullptr;
-    cudaError_t e = cudaMalloc(&p_, count * sizeof(T) + 64);
+    cudaError_t e = lib_malloc(&p_, count * sizeof(T) + 64);
     if (e != cudaSuccess) return fail(SWM_ERR_ALLOC, std::string("cudaMalloc: ") + cudaGetErrorString(e));
     cudaMemset(p_, 0, count * sizeof(T) + 64);
     allocs.push_back(p_);
@@ -374,17 +408,40 @@ static int enqueue_explicit(swm_solver* s) {
   return SWM_OK;
 }
 
+// LambdaMax and the non-finite/negative-depth flag of the state (TimeStep's
+// reduction, equation.f90:791-837), into s->lam / s->bad.
+static int enqueue_dt(swm_solver* s) {
+  CK(cudaMemsetAsync(s->lam, 0, 3 * sizeof(unsigned long long), s->stream));
+  DtArgs a{s->nx, s->ny, s->p.g, s->h, s->hu, s->hv, s->lam, s->bad};
+  CK(launch_dt(a, s->stream));
+  return SWM_OK;
+}
+
+static int enqueue_patankar(swm_solver* s);
+
+// One step: the scheme's launches, then the reduction of the new state, so that a
+// non-finite value born inside the step is reported by the step itself and the next
+// TimeStep() needs no launch of its own.  The Jacobi control block is cleared first:
+// every step starts from a clean barrier and residual state, also after a solve
+// that gave up on its grid barrier.
 static int enqueue_step(swm_solver* s) {
+  CK(cudaMemsetAsync(s->ctl, 0, sizeof(JacobiCtl), s->stream));
+  int rc;
   if (s->p.timescheme <= 4) {
-    CK(cudaMemsetAsync(&s->ctl->iters[0], 0, sizeof(int) * (kMaxSolves + 1), s->stream));
     s->n_solves = 0;
-    return enqueue_explicit(s);
+    rc = enqueue_explicit(s);
+  } else {
+    rc = enqueue_patankar(s);
   }
+  if (rc) return rc;
+  return enqueue_dt(s);
+}
+
+static int enqueue_patankar(swm_solver* s) {
   const bool two = (s->p.timescheme != 5);  // mPDeC2 or mPEuler: MSteps = 2
   const int ms = two ? 2 : 4, kc = two ? (s->p.timescheme == 7 ? 2 : 1) : 5;
   const bool csr = (s->p.solver == SWM_SOLVER_CSR);
   const bool compat = two && s->p.mpdec2_compat;
-  CK(cudaMemsetAsync(&s->ctl->iters[0], 0, sizeof(int) * (kMaxSolves + 1), s->stream));
   // RHS at U^n (timediscretization.f90:519), stored in slot 1 and used for all r at k=1
   prof_mark(s, 0);
   CK(launch_rhs(s, make_rhs_args(s, s->h, s->hu, s->hv, 0)));
@@ -483,7 +540,7 @@ static int enqueue_step(swm_solver* s) {
       ja.ctl = s->ctl;
       ja.block = jacobi_block_of(s->p);
       ja.recip = fast_patankar(s->p) ? 1 : 0;
-      ja.spin_limit = 1LL << 26;
+      ja.spin_limit = s->spin_limit;
       prof_mark(s, 2);
       CK(launch_jacobi(ja, csr, s->jac_blocks, s->stream));
       prof_mark(s, -1);
@@ -647,18 +704,18 @@ int swm_create(const swm_params* p, swm_handle* out) {
     AL(s->swb, 3 * N);
   }
   AL(s->dt_dev, 1);
-  AL(s->lam, 2);
-  AL(s->bad, 1);
+  AL(s->lam, 3);
+  s->bad = reinterpret_cast<int*>(s->lam + 2);
   AL(s->ctl, 1);
   AL(s->summary, 2 + 512);
   AL(s->stage, 3 * (nx + 6) * (ny + 6));
   AL(s->stage2, 3 * (nx + 6) * (ny + 6));
 #undef AL
-  if (cudaMallocHost(&s->h_dt, sizeof(double)) != cudaSuccess ||
-      cudaMallocHost(&s->h_ctl, sizeof(JacobiCtl)) != cudaSuccess ||
-      cudaMallocHost(&s->h_lam, 2 * sizeof(unsigned long long)) != cudaSuccess ||
-      cudaMallocHost(&s->h_bad, sizeof(int)) != cudaSuccess)
+  if (lib_malloc_host((void**)&s->h_dt, sizeof(double)) != cudaSuccess ||
+      lib_malloc_host((void**)&s->h_ctl, sizeof(JacobiCtl)) != cudaSuccess ||
+      lib_malloc_host((void**)&s->h_lam, 3 * sizeof(unsigned long long)) != cudaSuccess)
     return cleanup(fail(SWM_ERR_ALLOC, "cudaMallocHost failed"));
+  s->h_bad = reinterpret_cast<int*>(s->h_lam + 2);
 
   if (csr) {  // finitevolume.f90:219-267 CSR pattern, 1-based, slot order S, W, C, E, N
     std::vector<int> rs(N + 1), cl(5 * N);
@@ -739,7 +796,6 @@ int swm_destroy(swm_handle s) {
   if (s->h_dt) cudaFreeHost(s->h_dt);
   if (s->h_ctl) cudaFreeHost(s->h_ctl);
   if (s->h_lam) cudaFreeHost(s->h_lam);
-  if (s->h_bad) cudaFreeHost(s->h_bad);
   if (s->out_dev) cudaFree(s->out_dev);
   if (s->out_host) cudaFreeHost(s->out_host);
   if (s->stream) cudaStreamDestroy(s->stream);
@@ -761,6 +817,7 @@ int swm_set_state(swm_handle s, const double* U) {
   int rc = upload_ghosted(s, U, s->h, s->hu, s->hv);
   if (rc) return rc;
   s->have_state = true;
+  s->lam_fresh = false;
   return SWM_OK;
 }
 
@@ -785,6 +842,7 @@ int swm_set_planes(swm_handle s, const double* P) {
   CK(cudaMemcpyAsync(s->hv, P + 2 * s->N, s->N * sizeof(double), cudaMemcpyHostToDevice, s->stream));
   CK(cudaStreamSynchronize(s->stream));
   s->have_state = true;
+  s->lam_fresh = false;
   return SWM_OK;
 }
 
@@ -827,6 +885,7 @@ int swm_fill_ic(swm_handle s, int ic, const double* par, int npar) {
   CK(launch_ic_fill(a, s->stream));
   CK(cudaStreamSynchronize(s->stream));
   s->have_state = true;
+  s->lam_fresh = false;
   return SWM_OK;
 }
 
@@ -875,8 +934,8 @@ static int out_buffers(swm_solver* s, size_t bytes) {
   s->out_dev = nullptr;
   s->out_host = nullptr;
   s->out_cap = 0;
-  if (cudaMalloc(&s->out_dev, bytes) != cudaSuccess ||
-      cudaMallocHost(&s->out_host, bytes) != cudaSuccess)
+  if (lib_malloc((void**)&s->out_dev, bytes) != cudaSuccess ||
+      lib_malloc_host((void**)&s->out_host, bytes) != cudaSuccess)
     return fail(SWM_ERR_ALLOC, "output line buffers");
   s->out_cap = bytes;
   return SWM_OK;
@@ -1077,14 +1136,14 @@ int swm_timestep(swm_handle s, double* dt_min) {
   if (!s || !dt_min) return fail(SWM_ERR_PARAM, "null argument");
   if (!s->have_state) return fail(SWM_ERR_STATE, "no state set");
   CK(cudaSetDevice(s->device));
-  CK(cudaMemsetAsync(s->lam, 0, 2 * sizeof(unsigned long long), s->stream));
-  CK(cudaMemsetAsync(s->bad, 0, sizeof(int), s->stream));
-  DtArgs a{s->nx, s->ny, s->p.g, s->h, s->hu, s->hv, s->lam, s->bad};
-  CK(launch_dt(a, s->stream));
-  CK(cudaMemcpyAsync(s->h_lam, s->lam, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
-                     s->stream));
-  CK(cudaMemcpyAsync(s->h_bad, s->bad, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
-  CK(cudaStreamSynchronize(s->stream));
+  if (!s->lam_fresh) {  // the state changed since the last step's reduction
+    int rc = enqueue_dt(s);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(s->h_lam, s->lam, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                       s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    s->lam_fresh = true;
+  }
   double LX, LY;
   std::memcpy(&LX, &s->h_lam[0], sizeof(double));
   std::memcpy(&LY, &s->h_lam[1], sizeof(double));
@@ -1121,7 +1180,10 @@ int swm_step(swm_handle s, double t, double dt) {
     if (rc) return rc;
   }
   CK(cudaMemcpyAsync(s->h_ctl, s->ctl, sizeof(JacobiCtl), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaMemcpyAsync(s->h_lam, s->lam, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                     s->stream));
   CK(cudaStreamSynchronize(s->stream));
+  s->lam_fresh = true;
   if (s->n_solves == 0) {  // graph built without a host pass: count solves
     s->n_solves = solves_per_step(s->p.timescheme);
   }
@@ -1139,6 +1201,10 @@ int swm_step(swm_handle s, double t, double dt) {
   st.steps++;
   st.status = c.status;
   if (c.status < 0) return fail(SWM_ERR_WATCHDOG, "Jacobi grid barrier watchdog expired");
+  if (*s->h_bad) {
+    st.status = SWM_ERR_NAN;
+    return fail(SWM_ERR_NAN, "the step produced a non-finite value or a negative depth");
+  }
   if (c.status == 1) {
     g_last_error = "Jacobi not converged (maxIter reached)";
     return SWM_WARN_JACOBI_MAXITER;
@@ -1192,6 +1258,7 @@ int swm_profile_step(swm_handle s, double t, double dt, float* ms, int* launches
   }
   ms[3] = tot;
   CK(cudaMemcpy(s->h_ctl, s->ctl, sizeof(JacobiCtl), cudaMemcpyDeviceToHost));
+  s->lam_fresh = false;
   for (int k = 0; k < s->n_solves && k < kMaxSolves; ++k) s->stats.jacobi_iters[k] = s->h_ctl->iters[k];
   s->stats.n_solves = s->n_solves;
   return s->h_ctl->status < 0 ? fail(SWM_ERR_WATCHDOG, "watchdog") : SWM_OK;
@@ -1350,7 +1417,7 @@ int swm_debug_jacobi(swm_handle s, const double* mass, const double* diag, const
     CK(cudaMemcpy(s->cN, pl.data() + 3 * N, N * sizeof(double), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(s->cD, pl.data() + 4 * N, N * sizeof(double), cudaMemcpyHostToDevice));
   }
-  CK(cudaMemset(&s->ctl->iters[0], 0, sizeof(int) * (kMaxSolves + 1)));
+  CK(cudaMemset(s->ctl, 0, sizeof(JacobiCtl)));
   JacobiArgs ja{};
   ja.nx = s->nx;
   ja.ny = s->ny;
@@ -1373,7 +1440,7 @@ int swm_debug_jacobi(swm_handle s, const double* mass, const double* diag, const
   ja.ctl = s->ctl;
   ja.block = jacobi_block_of(s->p);
   ja.recip = fast_patankar(s->p) ? 1 : 0;
-  ja.spin_limit = 1LL << 26;
+  ja.spin_limit = s->spin_limit;
   CK(launch_jacobi(ja, csr, s->jac_blocks, s->stream));
   CK(cudaStreamSynchronize(s->stream));
   CK(cudaMemcpy(sol, out, N * sizeof(double), cudaMemcpyDeviceToHost));
@@ -1382,6 +1449,21 @@ int swm_debug_jacobi(swm_handle s, const double* mass, const double* diag, const
   if (iters) *iters = c.iters[0];
   if (c.status < 0) return fail(SWM_ERR_WATCHDOG, "Jacobi grid barrier watchdog expired");
   return c.status == 1 ? SWM_WARN_JACOBI_MAXITER : SWM_OK;
+}
+
+int swm_debug_set_spin_limit(swm_handle s, long long limit) {
+  if (!s) return fail(SWM_ERR_PARAM, "null handle");
+  s->spin_limit = limit;
+  drop_graph(s);  // the step graph bakes the limit into its Jacobi launches
+  return SWM_OK;
+}
+
+int swm_debug_inject_alloc_failure(long long nth, long long* counted) {
+  if (nth < 0) return fail(SWM_ERR_PARAM, "nth must be >= 0");
+  const long long n = g_alloc_count.exchange(0);
+  if (counted) *counted = n;
+  g_alloc_fail_at.store(nth);
+  return SWM_OK;
 }
 
 }  // extern "C"

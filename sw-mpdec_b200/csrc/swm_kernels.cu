@@ -587,7 +587,7 @@ __device__ bool grid_barrier(C* ctl, long long spin_limit, int* s_ok) {
     } else {
       long long spins = 0;
       while (*vgen == gen) {
-        if (++spins > spin_limit) {
+        if (++spins > spin_limit || spin_limit <= 0) {
           ok = 0;
           atomicExch(&ctl->status, -4);
           break;

@@ -15,6 +15,9 @@ namespace swm {
 constexpr int kResSlots = 3;    // ring of pass slots (see jacobi kernels)
 constexpr int kMaxBlock = 8;    // max Jacobi sweeps per stencil pass
 constexpr int kMaxSolves = 16;  // solves recorded per step
+// Polls of a grid-barrier wait before it gives up (status -4); ~1 s at 40 ns a poll.
+// A limit <= 0 makes every wait that is not already open give up at once.
+constexpr long long kDefaultSpinLimit = 1LL << 26;
 
 struct JacobiCtl {
   unsigned long long acc[kResSlots][kMaxBlock + 1][3];  // [slot][0 = initial, 1..T sweeps][limb]

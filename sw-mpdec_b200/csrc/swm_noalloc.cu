@@ -9,6 +9,7 @@
 // keeps its only scratch -- one iterate buffer and the solver's control block --
 // in the file-scope array below, which every GPU that loads this library holds
 // until the process exits.
+#include <cstdint>
 #include <mutex>
 
 #include "../../include/swm.h"
@@ -60,13 +61,34 @@ int swm_jacobi_noalloc(int nx, int ny, const double* cS, const double* cW, const
                         "nx*ny exceeds the 1048576-cell scratch of swm_jacobi_noalloc");
   if (!cS || !cW || !cE || !cN || !cD || !rhs || !sol)
     return noalloc_fail(SWM_ERR_PARAM, "null device array");
-  if (rhs == sol) return noalloc_fail(SWM_ERR_PARAM, "rhs and sol must not overlap");
+  // sol is written during the solve (it doubles as an iterate buffer) while the six
+  // inputs are read, so its byte range must not intersect any of theirs.
+  {
+    const size_t bytes = (size_t)nx * (size_t)ny * sizeof(double);
+    const uintptr_t s0 = reinterpret_cast<uintptr_t>(sol), s1 = s0 + bytes;
+    const double* in[6] = {cS, cW, cE, cN, cD, rhs};
+    for (const double* q : in) {
+      const uintptr_t q0 = reinterpret_cast<uintptr_t>(q), q1 = q0 + bytes;
+      if (q0 < s1 && s0 < q1)
+        return noalloc_fail(SWM_ERR_PARAM, "sol must not overlap rhs or a coefficient plane");
+    }
+  }
   if (maxiter < 1 || !(tol >= 0.0)) return noalloc_fail(SWM_ERR_PARAM, "maxiter >= 1, tol >= 0");
   if (block < 1 || block > swm::kMaxBlock) return noalloc_fail(SWM_ERR_PARAM, "block in 1..8");
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
     return noalloc_fail(SWM_ERR_CUDA, "no current CUDA device");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
+  // The call ends by synchronising `st` to read the iteration count, which a stream
+  // under capture cannot do (and doing it would invalidate the caller's capture).
+  {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+      cudaGetLastError();
+      return noalloc_fail(SWM_ERR_STATE,
+                          "swm_jacobi_noalloc synchronises its stream: not callable during capture");
+    }
+  }
 
   // Once per device, with that device current: the device address of the scratch
   // array (its host-side name is only a stand-in) and the persistent grid size.
@@ -111,7 +133,7 @@ int swm_jacobi_noalloc(int nx, int ny, const double* cS, const double* cW, const
   ja.out = sol;
   ja.ctl = ctl;
   ja.block = block;
-  ja.spin_limit = 1LL << 26;
+  ja.spin_limit = swm::kDefaultSpinLimit;
   e = swm::launch_jacobi(ja, false, ds.blocks[block], st);
   if (e != cudaSuccess) return noalloc_fail(SWM_ERR_CUDA, cudaGetErrorString(e));
   int res[2] = {0, 0};  // iters[0], status

@@ -29,7 +29,7 @@ EXPORTS = [
     "swm_batch_set_planes", "swm_batch_get_planes", "swm_batch_step", "swm_batch_cells",
     "swm_jacobi_noalloc", "swm_batch_get_stats", "swm_batch_get_stream",
     "swm_fill_ic", "swm_init_wb_ic", "swm_l1_error", "swm_write_output", "swm_write_mesh",
-    "swm_debug_format",
+    "swm_debug_format", "swm_debug_set_spin_limit", "swm_debug_inject_alloc_failure",
 ]
 
 
@@ -105,6 +105,8 @@ def load():
                                      P(ctypes.c_int)]
     lib.swm_debug_rhs.argtypes = [vp, dp, dp, dp, dp, dp]
     lib.swm_debug_jacobi.argtypes = [vp, dp, dp, dp, dp, P(ctypes.c_int)]
+    lib.swm_debug_set_spin_limit.argtypes = [vp, ctypes.c_longlong]
+    lib.swm_debug_inject_alloc_failure.argtypes = [ctypes.c_longlong, P(ctypes.c_longlong)]
     lib.swm_batch_create.argtypes = [ctypes.c_int, P(SwmParams), P(vp)]
     lib.swm_batch_destroy.argtypes = [vp]
     lib.swm_batch_set_planes.argtypes = [vp, ctypes.c_int, dp]
@@ -290,6 +292,10 @@ class Solver:
         _check(self.lib.swm_debug_rhs(self.h, _dp(U), _dp(Ut), _dp(FX), _dp(FY), _dp(S)))
         return dict(Ut=Ut, FX=FX, FY=FY, S=S)
 
+    def set_spin_limit(self, limit):
+        """Polls of each Jacobi grid-barrier wait before SWM_ERR_WATCHDOG (<= 0: at once)."""
+        _check(self.lib.swm_debug_set_spin_limit(self.h, int(limit)))
+
     def debug_jacobi(self, mass, diag, rhs):
         n = self.nx * self.ny
         sol = np.zeros(n)
@@ -300,6 +306,14 @@ class Solver:
         rc = _check(self.lib.swm_debug_jacobi(self.h, _dp(mass), _dp(diag), _dp(rhs), _dp(sol),
                                               ctypes.byref(it)))
         return sol, it.value, rc
+
+
+def inject_alloc_failure(nth):
+    """Make the library's nth allocation from now fail (0: none); returns the number
+    of allocations counted since the previous call."""
+    n = ctypes.c_longlong()
+    _check(load().swm_debug_inject_alloc_failure(int(nth), ctypes.byref(n)))
+    return n.value
 
 
 def jacobi_noalloc(nx, ny, cS, cW, cE, cN, cD, rhs, sol, maxiter=1000, tol=1e-16, block=4,

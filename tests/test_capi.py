@@ -35,13 +35,11 @@ def test_library_exports_every_declared_symbol():
     assert set(declared()) <= exported
 
 
-def c_layout(struct, fields):
+def c_layout(struct, fields, d):
     prog = ["#include <stdio.h>", "#include <stddef.h>", f'#include "{HEADER}"', "int main(){",
             f'printf("%zu\\n", sizeof({struct}));']
     prog += [f'printf("%zu\\n", offsetof({struct}, {f}));' for f in fields]
     prog += ["return 0;}"]
-    d = os.path.join(ROOT, "_work", "layout")
-    os.makedirs(d, exist_ok=True)
     src, exe = os.path.join(d, f"{struct}.c"), os.path.join(d, f"{struct}.bin")
     open(src, "w").write("\n".join(prog))
     cc = "/usr/bin/gcc" if os.path.exists("/usr/bin/gcc") else "gcc"
@@ -52,9 +50,9 @@ def c_layout(struct, fields):
 
 @pytest.mark.parametrize("struct,cls", [("swm_params", swm.SwmParams),
                                         ("swm_stats", swm.SwmStats)])
-def test_struct_layout_matches_ctypes(struct, cls):
+def test_struct_layout_matches_ctypes(struct, cls, tmp_path):
     names = [f[0] for f in cls._fields_]
-    size, offs = c_layout(struct, names)
+    size, offs = c_layout(struct, names, str(tmp_path))
     assert size == ctypes.sizeof(cls)
     assert offs == [getattr(cls, n).offset for n in names]
 
