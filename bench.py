@@ -11,15 +11,19 @@ TimeStep() + one mPDeC5 step (13 RHS evaluations, 13 Patankar solves).
                copies the ghosted state host->device and back (swm_set_state /
                swm_get_state), as a Fortran driver keeping U on the host would
   roofline     dominant kernel, algorithmic bytes / CUDA-event time
-  cpu_baseline the CPU restatement (oracle, OpenMP build) on a bounded sample
+  accuracy     the island case at 256^2 up to t = 0.8 (the hump runs up and over the
+               dry island top): split vs FP64 GPU forms and, with the CPU leg, vs the
+               oracle on the same dt sequence -- L1 (sum |dU| dx dy), relative L1, L-inf
+  cpu_baseline the CPU restatement (oracle, OpenMP build, all host threads) timed on
+               the accuracy leg's run, plus one host core on a bounded sample
 
 Multi-GPU (--gpus N under torchrun): replicas only -- every rank steps its own
 copy of the workload on its GPU, no data-path collective; value = N * cells *
 steps / (max over ranks of the timed region).
 
 --impl reference times the reference's CPU path (the oracle restatement: the
-Fortran reference cannot be compiled in this image) on a bounded sample of the
-same workload with all host threads.
+Fortran reference cannot be compiled in this image) on the same workload (island
+2048^2) with all host threads.
 """
 import argparse
 import json
@@ -38,14 +42,21 @@ METRIC = "mPDeC5 cell-steps/s at 2048Â²: split-precision vs FP64 GPU at L1 err â
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
 
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the split
-# step's kernels from one ncu capture each at 2048x2048 (4,194,304 cells); the named
-# summary under profiles/ holds the command and the counters.  Scaled by cells for
-# other grid sizes (the traffic of these kernels grows with the cell count).
+# step's kernels, each from one earlier ncu capture at 2048x2048 (4,194,304 cells):
+# constants, not measured by this run.  Each names the commit of the capture; a kernel
+# changed after it makes the figure stale.  Scaled by cells for other grid sizes (the
+# traffic of these kernels grows with the cell count).
 NCU_TRAFFIC_2048 = {
-    "rhs": (101276672.0 + 91489792.0, "profiles/rhs_split_island2048.md"),
-    "patankar_assemble": (None, "profiles/assemble_split_island2048.md"),  # k = 1 launch only
-    "jacobi": (403459328.0 + 58311680.0, "profiles/jacobi_stencil4_split_island2048.md"),
+    "rhs": (101276672.0 + 91489792.0, "b350e1f"),
+    "jacobi": (403459328.0 + 58311680.0, "77d112e"),
 }
+
+# Accuracy leg: the island case (stated hump at x = 2) at 256^2 up to t = 0.8, by which
+# the hump has run up and over the dry island top (wetting and drying).  The split and
+# FP64 forms take the FP64 form's dt sequence; with the CPU leg on, the oracle takes it
+# too (that run is also the timed CPU baseline) and both are compared with it.
+ACC_N = 256
+ACC_T_END = 0.8
 
 # Algorithmic bytes per cell-step of the whole mPDeC5 step: every phase reads its
 # inputs and writes its outputs once (halo re-reads not counted), the Patankar
@@ -154,35 +165,96 @@ def timed_steps(s, torch, steps, warmup, on_start=None):
     return e0.elapsed_time(e1), iters
 
 
-def cpu_sample(steps=1, n=512):
-    """Oracle (OpenMP build) on the island case at n^2 (same domain and physics)."""
+def errors(a, b, c):
+    """Per variable (h, hu, hv): the reference's L1 error sum |a - b| dx dy
+    (postprocessing.f90:47,51), the relative L1 sum |a - b| / sum |b|, and L-infinity."""
+    dx = (c["x1"][0] - c["x0"][0]) / c["nx"]
+    dy = (c["x1"][1] - c["x0"][1]) / c["ny"]
+    d = np.abs(a - b)
+    return {"l1": [float(d[v].sum() * dx * dy) for v in range(3)],
+            "rel_l1": [float(d[v].sum() / max(np.abs(b[v]).sum(), 1e-300)) for v in range(3)],
+            "linf": [float(d[v].max()) for v in range(3)]}
+
+
+def accuracy_leg(swm, cases, with_cpu, block, device):
+    """Split and FP64 forms (and, in the CPU leg, the oracle) over a wet-dry horizon on
+    the same dt sequence; returns (accuracy, cpu_baseline or None)."""
+    c = cases.case("island", n=ACC_N)
+    planes = cases.cell_averages(c)
+    s64 = make_solver(swm, c, "fp64", block=block, device=device)
+    s64.set_planes(planes)
+    dts, t = [], 0.0
+    while ACC_T_END - t > 1e-12:
+        dt = min(s64.timestep(), ACC_T_END - t)
+        s64.step(t, dt)
+        dts.append(dt)
+        t += dt
+    p64 = s64.get_planes()
+    s64.close()
+    s32 = make_solver(swm, c, "split", block=block, device=device)
+    s32.set_planes(planes)
+    for dt in dts:
+        s32.step(0.0, dt)
+    p32 = s32.get_planes()
+    s32.close()
+    dry0 = int((planes[0] <= 1.0001e-6).sum())
+    acc = {"workload": f"island {ACC_N}x{ACC_N} (hump at x = 2) to t = {t:.3f}: the hump runs "
+                       f"up and over the dry island top", "steps": len(dts), "t_end": t,
+           "dry_cells_initial": dry0, "dry_cells_final": int((p64[0] <= 1.0001e-6).sum()),
+           "bar": "split-form L1 = sum |U - U_ref| dx dy (postprocessing.f90:47,51) <= 1e-6 "
+                  "per variable, U_ref the oracle (FP64)",
+           "split_vs_fp64": errors(p32, p64, c), "min_h_split": float(p32[0].min())}
+    if not with_cpu:
+        return acc, None
+    # --- CPU leg: the oracle (test infrastructure) is the timed CPU baseline and the
+    # accuracy reference of the same run
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import cases
     import oracle as O
-    c = cases.case("island", n=n)
-    p = O.make_params(c["nx"], c["ny"], c["x0"], c["x1"], g=c["g"], cfl=c["cfl"],
-                      bathy_flag=c["bathy_flag"], bathy_par=c["bathy_par"])
-    o = O.Oracle(p, threaded=True)
-    o.set_planes(cases.cell_averages(c))
-    dt = o.timestep()
-    o.step(0.0, dt)  # warm-up (page-in)
+    op = O.make_params(c["nx"], c["ny"], c["x0"], c["x1"], g=c["g"], cfl=c["cfl"],
+                       bathy_flag=c["bathy_flag"], bathy_par=c["bathy_par"])
+    o = O.Oracle(op, threaded=True)
+    o.set_planes(planes)
     t0 = time.perf_counter()
-    for _ in range(steps):
-        o.step(0.0, o.timestep())
+    for dt in dts:
+        o.timestep()
+        o.step(0.0, dt)
     el = time.perf_counter() - t0
-    return {"value": c["nx"] * c["ny"] * steps / el, "unit": "cell-steps/s",
-            "cores": O.threads(True), "kind": "port",
-            "sample": f"island case at {n}x{n} (same domain/physics), {steps} mPDeC5 step(s) "
-                      f"after 1 warm-up, CPU restatement of the Fortran (oracle/swm_oracle.c, "
-                      f"OpenMP build)"}
+    po = o.get_planes()
+    del o
+    acc["split_vs_oracle"] = errors(p32, po, c)
+    acc["fp64_vs_oracle"] = {"bitwise": bool(np.array_equal(p64, po)),
+                             "rel_l1": errors(p64, po, c)["rel_l1"]}
+    acc["pass"] = bool(max(acc["split_vs_oracle"]["l1"]) <= 1e-6)
+    cells = c["nx"] * c["ny"]
+    cpu = {"value": cells * len(dts) / el, "unit": "cell-steps/s", "cores": O.threads(True),
+           "kind": "port",
+           "sample": f"the accuracy leg's run: island {ACC_N}x{ACC_N}, {len(dts)} mPDeC5 steps "
+                     f"to t = {t:.3f}, CPU restatement of the Fortran (oracle/swm_oracle.c, "
+                     f"OpenMP build, all host threads)"}
+    # one host core: the serial build on 2 steps of the island case at 512^2
+    n1, k1 = 512, 2
+    c1 = cases.case("island", n=n1)
+    o1 = O.Oracle(O.make_params(c1["nx"], c1["ny"], c1["x0"], c1["x1"], g=c1["g"], cfl=c1["cfl"],
+                                bathy_flag=c1["bathy_flag"], bathy_par=c1["bathy_par"]))
+    o1.set_planes(cases.cell_averages(c1))
+    t0 = time.perf_counter()
+    for _ in range(k1):
+        o1.step(0.0, o1.timestep())
+    el1 = time.perf_counter() - t0
+    cpu["single_core"] = {"value": n1 * n1 * k1 / el1, "unit": "cell-steps/s", "cores": 1,
+                          "sample": f"island {n1}x{n1}, {k1} mPDeC5 steps, serial build"}
+    return acc, cpu
 
 
 def reference_arm(args, rank, world):
+    """The reference's CPU path on the arm's own workload (island at --n, default
+    2048^2): the oracle's OpenMP build on all host threads.  A step at 2048^2 takes
+    seconds on the CPU, so at most one warm-up step (page-in) is run."""
     if rank != 0:
         return
     os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
-    n = 512
-    warm = max(args.warmup, 0)
+    n = args.n
+    warm = min(max(args.warmup, 0), 1)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import cases
     import oracle as O
@@ -201,15 +273,15 @@ def reference_arm(args, rank, world):
     cores = O.threads(True)
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "cell-steps/s",
-        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": warm,
         "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"island {n}x{n} sample of the 2048x2048 wave-over-dry-island "
-                               f"case (same domain, bathymetry and hump), mPDeC5, CFL 0.4",
-                   "parallelism": "host threads"},
+        "config": {"workload": f"island {n}x{n} periodic (wave over dry island), mPDeC5, "
+                               f"CFL 0.4", "cells": n * n, "parallelism": "host threads"},
         "cpu_baseline": {"value": v, "unit": "cell-steps/s", "cores": cores, "kind": "port",
                          "sample": f"{args.steps} mPDeC5 steps of the island case at {n}x{n} "
-                                   f"after {warm} warm-up steps; the Fortran reference has no "
+                                   f"after {warm} warm-up step(s) (at most one: a step takes "
+                                   f"seconds on the CPU); the Fortran reference has no "
                                    f"compiler here, so its C restatement (oracle) is timed"},
         "e2e": {"value": v, "unit": "cell-steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
@@ -280,12 +352,11 @@ def main():
         s.close()
         del s
 
-    # accuracy of the split form against the FP64 form on the same steps
-    a, b = results["split"]["final"], results["fp64"]["final"]
-    l1 = [float(np.abs(a[v] - b[v]).sum() / max(np.abs(b[v]).sum(), 1e-300)) for v in range(3)]
-    area = (c["x1"][0] - c["x0"][0]) * (c["x1"][1] - c["x0"][1]) / cells
-    l1_abs = [float(np.abs(a[v] - b[v]).sum() * area) for v in range(3)]
-    hmin = float(a[0].min())
+    # the split form against the FP64 form after the timed steps (short horizon); the
+    # wet-dry accuracy leg against the oracle runs after the GPU legs
+    short = errors(results["split"]["final"], results["fp64"]["final"], c)
+    short["steps"] = args.steps + args.warmup
+    short["min_h_split"] = float(results["split"]["final"][0].min())
 
     # end to end through the C ABI with host buffers
     e2e = None
@@ -356,6 +427,14 @@ def main():
             dist.destroy_process_group()
         return
 
+    # accuracy over a wet-dry horizon; with the CPU leg, the oracle's run of it is the
+    # timed CPU baseline and the accuracy reference (rank 0 only, after all timing)
+    acc, cpu = None, None
+    try:
+        acc, cpu = accuracy_leg(swm, cases, world == 1 and not args.no_cpu, args.block, local)
+    except Exception as exc:  # a failed side leg must not hide the GPU number
+        acc = {"error": str(exc)}
+
     sp, fp = results["split"], results["fp64"]
     value = world * cells * args.steps / (sp["ms"] * 1e-3)
     value64 = world * cells * args.steps / (fp["ms"] * 1e-3)
@@ -380,8 +459,11 @@ def main():
         alg = 208.0 * cells
     t_launch = classes[dom][0] / max(classes[dom][1], 1) * 1e-3
     achieved = alg / t_launch / 1e9
-    tb, traffic_src = NCU_TRAFFIC_2048.get(dom, (None, None))
+    tb, traffic_commit = NCU_TRAFFIC_2048.get(dom, (None, None))
     traffic = tb * cells / 2048.0**2 if tb else None
+    traffic_src = (f"constant from one ncu capture (dram__bytes_read.sum + dram__bytes_write.sum, "
+                   f"one launch at 2048^2) at commit {traffic_commit}, scaled by cells; not "
+                   f"measured by this run" if tb else None)
     # whole-step byte model for both forms (N_J = measured Jacobi sweeps per step)
     step_rf = {"unit": "GB/s", "peak": peak, "jacobi_sweeps_per_step": nj,
                "bytes_per_cell_step": {}, "achieved": {}, "frac": {}}
@@ -403,9 +485,8 @@ def main():
         "fp64": {"value": value64, "ms_per_step": fp["ms"] / args.steps,
                  "jacobi_iters_per_step": fp["iters"] / args.steps},
         "split_over_fp64": value / value64,
-        "accuracy": {"rel_l1_split_vs_fp64_per_var": l1, "l1_split_vs_fp64_per_var": l1_abs,
-                     "min_h": hmin,
-                     "steps": args.steps + args.warmup},
+        "accuracy": acc,
+        "accuracy_timed_steps_split_vs_fp64": short,
         "jacobi_iters_per_step": nj,
         "kernel_ms_per_step": {k: v[0] for k, v in classes.items()},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
@@ -418,11 +499,8 @@ def main():
         "e2e": e2e,
         "ensemble": ens,
     }
-    if not args.no_cpu:
-        try:
-            line["cpu_baseline"] = cpu_sample()
-        except Exception as exc:  # the baseline must not hide the GPU number
-            line["cpu_baseline"] = {"value": None, "error": str(exc)}
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()

@@ -214,6 +214,10 @@ SWM_API int swm_debug_jacobi(swm_handle h, const double *mass, const double *dia
  * allocator had; 0 disables.  *counted (nullable) receives the number of
  * allocations made since the previous call. */
 SWM_API int swm_debug_set_spin_limit(swm_handle h, long long limit);
+/* RHS tile loads: enable = 1 (default) stages the haloed state tiles that lie inside
+ * the grid by TMA tensor copies (even nx), 0 loads every tile with wrapped-index
+ * loads.  Both give bit-identical results; the step's graph is rebuilt. */
+SWM_API int swm_debug_set_tma(swm_handle h, int enable);
 SWM_API int swm_debug_inject_alloc_failure(long long nth, long long *counted);
 
 /* ---- allocation-free Jacobi solve ----

@@ -16,6 +16,8 @@
 #include <string>
 #include <vector>
 
+#include <cudaTypedefs.h>
+
 #include "../../include/swm.h"
 #include "swm_host.h"
 #include "swm_kernels.cuh"
@@ -149,6 +151,9 @@ struct swm_solver {
   // the step's last launch computes LambdaMax and the non-finite/negative-depth flag
   // of the new state; swm_timestep uses them while the state is unchanged
   bool lam_fresh = false;
+  // TMA staging of the RHS tiles: tensor maps of every plane an RHS reads, by address
+  bool tma = true;
+  std::vector<std::pair<const double*, CUtensorMap>> tmaps;
   // per-launch event profiling (swm_profile_step)
   bool profiling = false;
   std::vector<cudaEvent_t> prof_ev;
@@ -223,12 +228,72 @@ static RhsArgs make_rhs_args(swm_solver* s, const double* h, const double* hu, c
   a.src_cols = s->src_cols;
   a.src_rows = s->src_rows;
   a.bgrad = s->bgrad;
+  a.status = &s->ctl->status;
   return a;
 }
 
+// cuTensorMapEncodeTiled from the driver, looked up once (no link against libcuda).
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static bool looked = false;
+  if (!looked) {
+    looked = true;
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    cudaGetLastError();
+  }
+  return fn;
+}
+
+// Tensor map of one [ny][nx] FP64 plane for the RHS tile box (kTmaBoxX x kTmaBoxY);
+// false when the plane cannot be described (row pitch not a multiple of 16 bytes,
+// base not 16-byte aligned, grid smaller than the box, no encoder).
+static bool plane_map(swm_solver* s, const double* base, CUtensorMap* out) {
+  for (const auto& e : s->tmaps)
+    if (e.first == base) {
+      *out = e.second;
+      return true;
+    }
+  auto enc = tensor_map_encoder();
+  if (!enc || (s->nx % 2) != 0 || (reinterpret_cast<uintptr_t>(base) & 15) != 0 ||
+      s->nx < kTmaBoxX || s->ny < kTmaBoxY)
+    return false;
+  const cuuint64_t dims[2] = {(cuuint64_t)s->nx, (cuuint64_t)s->ny};
+  const cuuint64_t strides[1] = {(cuuint64_t)s->nx * sizeof(double)};
+  const cuuint32_t box[2] = {(cuuint32_t)kTmaBoxX, (cuuint32_t)kTmaBoxY};
+  const cuuint32_t estr[2] = {1, 1};
+  CUtensorMap m;
+  if (enc(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double*>(base), dims, strides, box,
+          estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return false;
+  s->tmaps.emplace_back(base, m);
+  *out = m;
+  return true;
+}
+
 static cudaError_t launch_rhs(swm_solver* s, const RhsArgs& a) {
-  if (s->p.precision == SWM_PREC_FP64) return launch_rhs_exact(a, s->stream);
-  return launch_rhs_fast(s->p.precision == SWM_PREC_SPLIT ? 1 : 0, a, s->stream);
+  RhsTma tm;
+  std::memset(&tm, 0, sizeof(tm));
+  tm.enabled = s->tma && plane_map(s, a.h, &tm.plane[0]) && plane_map(s, a.hu, &tm.plane[1]) &&
+               plane_map(s, a.hv, &tm.plane[2]);
+  if (s->p.precision == SWM_PREC_FP64) return launch_rhs_exact(a, tm, s->stream);
+  return launch_rhs_fast(s->p.precision == SWM_PREC_SPLIT ? 1 : 0, a, tm, s->stream);
+}
+
+// One RHS outside a step, waited for: a tile whose TMA load gave up is reported.
+static int run_rhs_sync(swm_solver* s, const RhsArgs& a) {
+  CK(cudaMemsetAsync(&s->ctl->status, 0, sizeof(int), s->stream));
+  CK(launch_rhs(s, a));
+  int st = 0;
+  CK(cudaMemcpyAsync(&st, &s->ctl->status, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  if (st < 0) return fail(SWM_ERR_WATCHDOG, "an RHS tile load did not complete");
+  return SWM_OK;
 }
 
 static void fill_thresh(const swm_solver* s, unsigned long long t[3]) {
@@ -904,8 +969,8 @@ int swm_init_wb_ic(swm_handle s, int ic, const double* par, int npar) {
   a.fx_full = s->fxwb;
   a.fy_full = s->fywb;
   a.s_full = s->swb;
-  CK(launch_rhs(s, a));
-  CK(cudaStreamSynchronize(s->stream));
+  rc = run_rhs_sync(s, a);
+  if (rc) return rc;
   s->have_wb = true;
   drop_graph(s);  // the step graph bakes the WB pointers in
   return SWM_OK;
@@ -1125,8 +1190,8 @@ int swm_set_wb_state(swm_handle s, const double* Uwb) {
   a.fx_full = s->fxwb;
   a.fy_full = s->fywb;
   a.s_full = s->swb;
-  CK(launch_rhs(s, a));
-  CK(cudaStreamSynchronize(s->stream));
+  rc = run_rhs_sync(s, a);
+  if (rc) return rc;
   s->have_wb = true;
   drop_graph(s);  // the step graph bakes the WB pointers in
   return SWM_OK;
@@ -1349,8 +1414,8 @@ int swm_debug_rhs(swm_handle s, const double* U, double* Ut, double* FX, double*
   a.fy_full = dfy;
   a.s_full = ds;
   a.ut_h = dh;  // Ut(1), as the build without PATANKAR computes it
-  cudaError_t e = launch_rhs(s, a);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);  // s->stream is non-blocking
+  rc = run_rhs_sync(s, a);
+  cudaError_t e = rc ? cudaErrorUnknown : cudaSuccess;
   std::vector<double> hfx(3 * nfx), hfy(3 * nfy), hs(3 * N), hht(N), hut(N), hvt(N);
   if (e == cudaSuccess) e = cudaMemcpy(hht.data(), dh, N * sizeof(double), cudaMemcpyDeviceToHost);
   if (e == cudaSuccess) e = cudaMemcpy(hfx.data(), dfx, 3 * nfx * sizeof(double), cudaMemcpyDeviceToHost);
@@ -1362,6 +1427,7 @@ int swm_debug_rhs(swm_handle s, const double* U, double* Ut, double* FX, double*
   cudaFree(dfy);
   cudaFree(ds);
   cudaFree(dh);
+  if (rc) return rc;
   if (e != cudaSuccess) return fail(SWM_ERR_CUDA, cudaGetErrorString(e));
   // to the reference's column-major (3, ., .) layouts
   for (size_t j = 0; j < ny; ++j)
@@ -1449,6 +1515,13 @@ int swm_debug_jacobi(swm_handle s, const double* mass, const double* diag, const
   if (iters) *iters = c.iters[0];
   if (c.status < 0) return fail(SWM_ERR_WATCHDOG, "Jacobi grid barrier watchdog expired");
   return c.status == 1 ? SWM_WARN_JACOBI_MAXITER : SWM_OK;
+}
+
+int swm_debug_set_tma(swm_handle s, int enable) {
+  if (!s) return fail(SWM_ERR_PARAM, "null handle");
+  s->tma = enable != 0;
+  drop_graph(s);
+  return SWM_OK;
 }
 
 int swm_debug_set_spin_limit(swm_handle s, long long limit) {

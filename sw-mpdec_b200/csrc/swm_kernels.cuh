@@ -166,8 +166,8 @@ cudaError_t launch_jacobi_batch(const JacobiBatchArgs& a, int grid_blocks, bool 
 int jacobi_batch_grid_blocks(int block, int device, bool recip);
 cudaError_t launch_dt_batch(const DtBatchDesc* d, const int2* blk, int nblk, int nprob,
                             unsigned long long* lam, int* bad, double* dt, cudaStream_t s);
-cudaError_t launch_rhs_fast(int mode, const RhsArgs& a, cudaStream_t s);
-cudaError_t launch_rhs_exact(const RhsArgs& a, cudaStream_t s);
+cudaError_t launch_rhs_fast(int mode, const RhsArgs& a, const RhsTma& tm, cudaStream_t s);
+cudaError_t launch_rhs_exact(const RhsArgs& a, const RhsTma& tm, cudaStream_t s);
 size_t rhs_smem_bytes(int mode);
 
 cudaError_t launch_dt(const DtArgs& a, cudaStream_t s);

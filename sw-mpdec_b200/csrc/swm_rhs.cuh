@@ -21,6 +21,7 @@
 #include <type_traits>
 
 #include "swm_device.cuh"
+#include "swm_tma.cuh"
 
 namespace swm {
 
@@ -60,6 +61,8 @@ struct RhsArgs {
   // nullable: b_x, b_y at the 16 interior Gauss points of every cell, evaluated on the
   // host with the analytic formula (equation.f90:451-509), planes [4][4][2][ny*nx]
   const double* bgrad;
+  // nullable: status word set to -4 when a tile's TMA load did not complete in time
+  int* status;
 };
 
 // 16 x 16 tiles: less vertical halo than 32 x 8 (the FP64 form is 4% faster, the split
@@ -160,14 +163,17 @@ __device__ __forceinline__ void store_mp(unsigned long long* p, int pitch, f2 wm
 }
 
 // MODE: 0 FP64 (EXACT per translation unit), 1 SPLIT.  One CTA, tile origin (i0, j0).
+// tm (nullable): tensor maps of the input planes; tiles whose haloed box lies inside
+// the grid are then staged by TMA, the others (at the periodic seams) by wrapped loads.
 template <int MODE>
-__device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const int j0) {
+__device__ __forceinline__ void rhs_tile(const RhsArgs& a, const RhsTma* tm, const int i0,
+                                         const int j0) {
   using T = typename std::conditional<MODE == 1, float, double>::type;
   constexpr bool EX = (MODE == 0) && SWM_EXACT;
   constexpr int TX = RHS_TX, TY = RHS_TY, NT = RHS_NT;
   using SM = RhsSmem<T>;
   constexpr int VX = SM::VX, VY = SM::VY;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   double* sV = reinterpret_cast<double*>(smem_raw);  // [3][VY][VX]
   double* sW = sV + SM::nV;                          // [2][3][4][cells]
   double* sFX = sW + SM::nW;                         // [3][TY][TX+1]
@@ -181,27 +187,63 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const i
   const int tid = threadIdx.x;
 
   // ---- load the haloed tile, V = ConsToPrim(U) (equation.f90:778-782) ----
-  // Periodic wrap: one conditional add/subtract when the grid is at least one haloed
-  // tile wide, the general modulo otherwise.
-  const bool wide = nx >= VX && ny >= VY;
   constexpr int NLD = (VY * VX + NT - 1) / NT;  // cells per thread; all loads issued first
   double lh[NLD], lhu[NLD], lhv[NLD];
+  static_assert(kTmaBoxX >= VX + 1 && kTmaBoxY == VY, "TMA box covers the haloed tile");
+  static_assert(3 * kTmaBoxX * kTmaBoxY + 16 <= SM::nW, "TMA staging fits the face-value area");
+  if (tm != nullptr && tm->enabled && i0 >= 4 && i0 - 4 + kTmaBoxX <= nx && j0 >= 3 &&
+      j0 - 3 + kTmaBoxY <= ny) {
+    // Interior tile: one thread copies the three 24 x 22 boxes (columns i0-4..i0+19,
+    // rows j0-3..j0+18) into the face-value area, unused until the x second sweeps,
+    // rounded up to a 128-byte boundary; every thread waits on the barrier.
+    __shared__ __align__(8) uint64_t s_bar;
+    const unsigned sw0 = smem_u32(sW);
+    double* stg = sW + (((sw0 + 127u) & ~127u) - sw0) / sizeof(double);
+    if (tid == 0) mbar_init(&s_bar, 1);
+    __syncthreads();
+    if (tid == 0) {
+      mbar_arrive_expect_tx(&s_bar, 3 * kTmaBoxBytes);
 #pragma unroll
-  for (int q = 0; q < NLD; ++q) {
-    const int it = tid + q * NT;
-    if (it < VY * VX) {
-      int gi = i0 - 3 + it % VX, gj = j0 - 3 + it / VX;
-      if (wide) {
-        gi += gi < 0 ? nx : (gi >= nx ? -nx : 0);
-        gj += gj < 0 ? ny : (gj >= ny ? -ny : 0);
-      } else {
-        gi = wrap(gi, nx);
-        gj = wrap(gj, ny);
+      for (int v = 0; v < 3; ++v)
+        tma_load_2d(stg + v * kTmaBoxX * kTmaBoxY, &tm->plane[v], i0 - 4, j0 - 3, &s_bar);
+    }
+    const bool ok = mbar_wait_bounded(&s_bar, 0, kTmaWaitLimit);
+    if (__syncthreads_or(!ok)) {  // the copy did not complete: report and give up the tile
+      if (tid == 0 && a.status) atomicExch(a.status, -4);
+      mbar_wait_bounded(&s_bar, 0, kTmaWaitLimit);  // bounded wait for the copies in flight
+      return;
+    }
+#pragma unroll
+    for (int q = 0; q < NLD; ++q) {
+      const int it = tid + q * NT;
+      if (it < VY * VX) {
+        const int k = (it / VX) * kTmaBoxX + it % VX + 1;
+        lh[q] = stg[k];
+        lhu[q] = stg[kTmaBoxX * kTmaBoxY + k];
+        lhv[q] = stg[2 * kTmaBoxX * kTmaBoxY + k];
       }
-      const size_t k = (size_t)gj * nx + gi;
-      lh[q] = a.h[k];
-      lhu[q] = a.hu[k];
-      lhv[q] = a.hv[k];
+    }
+  } else {
+    // Periodic wrap: one conditional add/subtract when the grid is at least one haloed
+    // tile wide, the general modulo otherwise.
+    const bool wide = nx >= VX && ny >= VY;
+#pragma unroll
+    for (int q = 0; q < NLD; ++q) {
+      const int it = tid + q * NT;
+      if (it < VY * VX) {
+        int gi = i0 - 3 + it % VX, gj = j0 - 3 + it / VX;
+        if (wide) {
+          gi += gi < 0 ? nx : (gi >= nx ? -nx : 0);
+          gj += gj < 0 ? ny : (gj >= ny ? -ny : 0);
+        } else {
+          gi = wrap(gi, nx);
+          gj = wrap(gj, ny);
+        }
+        const size_t k = (size_t)gj * nx + gi;
+        lh[q] = a.h[k];
+        lhu[q] = a.hu[k];
+        lhv[q] = a.hv[k];
+      }
     }
   }
 #pragma unroll
@@ -674,8 +716,9 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const int i0, const i
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(RHS_NT, 2) rhs_kernel(const RhsArgs a) {
-  rhs_tile<MODE>(a, blockIdx.x * RHS_TX, blockIdx.y * RHS_TY);
+__global__ void __launch_bounds__(RHS_NT, 2)
+    rhs_kernel(const RhsArgs a, const __grid_constant__ RhsTma tm) {
+  rhs_tile<MODE>(a, &tm, blockIdx.x * RHS_TX, blockIdx.y * RHS_TY);
 }
 
 // Ensembles: CTA b computes tile (work[b].y, work[b].z) of problem work[b].x, whose
@@ -690,7 +733,7 @@ __global__ void __launch_bounds__(RHS_NT, 2)
     reinterpret_cast<unsigned long long*>(&sa)[threadIdx.x] =
         reinterpret_cast<const unsigned long long*>(&descs[w.x])[threadIdx.x];
   __syncthreads();
-  rhs_tile<MODE>(sa, w.y, w.z);
+  rhs_tile<MODE>(sa, nullptr, w.y, w.z);
 }
 
 }  // namespace SWM_RHS_NS

@@ -8,7 +8,7 @@
 
 namespace swm {
 
-cudaError_t launch_rhs_exact(const RhsArgs& a, cudaStream_t s) {
+cudaError_t launch_rhs_exact(const RhsArgs& a, const RhsTma& tm, cudaStream_t s) {
   dim3 grd((a.gr.nx + RHS_TX - 1) / RHS_TX, (a.gr.ny + RHS_TY - 1) / RHS_TY);
   size_t sm = RhsSmem<double>::bytes;
   static bool attr = false;
@@ -17,7 +17,7 @@ cudaError_t launch_rhs_exact(const RhsArgs& a, cudaStream_t s) {
                          (int)sm);
     attr = true;
   }
-  rhs_exact::rhs_kernel<0><<<grd, RHS_NT, sm, s>>>(a);
+  rhs_exact::rhs_kernel<0><<<grd, RHS_NT, sm, s>>>(a, tm);
   return cudaGetLastError();
 }
 

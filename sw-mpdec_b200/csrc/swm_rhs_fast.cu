@@ -10,7 +10,7 @@ size_t rhs_smem_bytes(int mode) {
   return mode == 1 ? RhsSmem<float>::bytes : RhsSmem<double>::bytes;
 }
 
-cudaError_t launch_rhs_fast(int mode, const RhsArgs& a, cudaStream_t s) {
+cudaError_t launch_rhs_fast(int mode, const RhsArgs& a, const RhsTma& tm, cudaStream_t s) {
   dim3 grd((a.gr.nx + RHS_TX - 1) / RHS_TX, (a.gr.ny + RHS_TY - 1) / RHS_TY);
   if (mode == 1) {
     size_t sm = RhsSmem<float>::bytes;
@@ -20,7 +20,7 @@ cudaError_t launch_rhs_fast(int mode, const RhsArgs& a, cudaStream_t s) {
                            (int)sm);
       attr = true;
     }
-    rhs_fast::rhs_kernel<1><<<grd, RHS_NT, sm, s>>>(a);
+    rhs_fast::rhs_kernel<1><<<grd, RHS_NT, sm, s>>>(a, tm);
   } else {
     size_t sm = RhsSmem<double>::bytes;
     static bool attr = false;
@@ -29,7 +29,7 @@ cudaError_t launch_rhs_fast(int mode, const RhsArgs& a, cudaStream_t s) {
                            (int)sm);
       attr = true;
     }
-    rhs_fast::rhs_kernel<0><<<grd, RHS_NT, sm, s>>>(a);
+    rhs_fast::rhs_kernel<0><<<grd, RHS_NT, sm, s>>>(a, tm);
   }
   return cudaGetLastError();
 }

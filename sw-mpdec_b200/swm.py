@@ -30,6 +30,7 @@ EXPORTS = [
     "swm_jacobi_noalloc", "swm_batch_get_stats", "swm_batch_get_stream",
     "swm_fill_ic", "swm_init_wb_ic", "swm_l1_error", "swm_write_output", "swm_write_mesh",
     "swm_debug_format", "swm_debug_set_spin_limit", "swm_debug_inject_alloc_failure",
+    "swm_debug_set_tma",
 ]
 
 
@@ -106,6 +107,7 @@ def load():
     lib.swm_debug_rhs.argtypes = [vp, dp, dp, dp, dp, dp]
     lib.swm_debug_jacobi.argtypes = [vp, dp, dp, dp, dp, P(ctypes.c_int)]
     lib.swm_debug_set_spin_limit.argtypes = [vp, ctypes.c_longlong]
+    lib.swm_debug_set_tma.argtypes = [vp, ctypes.c_int]
     lib.swm_debug_inject_alloc_failure.argtypes = [ctypes.c_longlong, P(ctypes.c_longlong)]
     lib.swm_batch_create.argtypes = [ctypes.c_int, P(SwmParams), P(vp)]
     lib.swm_batch_destroy.argtypes = [vp]
@@ -291,6 +293,10 @@ class Solver:
         S = np.zeros((ny, nx, 3))
         _check(self.lib.swm_debug_rhs(self.h, _dp(U), _dp(Ut), _dp(FX), _dp(FY), _dp(S)))
         return dict(Ut=Ut, FX=FX, FY=FY, S=S)
+
+    def set_tma(self, enable):
+        """RHS tile loads by TMA (True, default) or by wrapped-index loads (False)."""
+        _check(self.lib.swm_debug_set_tma(self.h, 1 if enable else 0))
 
     def set_spin_limit(self, limit):
         """Polls of each Jacobi grid-barrier wait before SWM_ERR_WATCHDOG (<= 0: at once)."""
