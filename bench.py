@@ -138,11 +138,17 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def make_solver(swm, c, precision, solver="stencil", block=4, device=0):
+def make_solver(swm, c, precision, solver="stencil", block=4, device=0, source_table=1):
     return swm.Solver(nx=c["nx"], ny=c["ny"], x0=c["x0"], x1=c["x1"], g=c["g"], cfl=c["cfl"],
                       bathy_flag=c["bathy_flag"], bathy_par=c["bathy_par"],
                       well_balanced=c["well_balanced"], precision=precision, solver=solver,
-                      jacobi_block=block, device=device)
+                      jacobi_block=block, device=device, source_table=source_table)
+
+
+# Timed forms: the split form (the metric's numerator) and the plain FP64 form twice,
+# with the bathymetry source from the per-cell gradient table (bit-identical to the
+# oracle) and from the per-column/row factors (within 1e-12 of it, no per-cell table).
+FORMS = {"fp64": ("fp64", 1), "fp64_factored": ("fp64", 0), "split": ("split", 1)}
 
 
 def timed_steps(s, torch, steps, warmup, on_start=None):
@@ -334,8 +340,8 @@ def main():
 
     results = {}
     clocks = None
-    for prec in ("fp64", "split"):
-        s = make_solver(swm, c, prec, block=args.block, device=local)
+    for prec, (form, table) in FORMS.items():
+        s = make_solver(swm, c, form, block=args.block, device=local, source_table=table)
         s.set_planes(planes)
         barrier()
         sampler = ClockSampler(local) if prec == "split" else None
@@ -438,6 +444,11 @@ def main():
     sp, fp = results["split"], results["fp64"]
     value = world * cells * args.steps / (sp["ms"] * 1e-3)
     value64 = world * cells * args.steps / (fp["ms"] * 1e-3)
+    ff = results["fp64_factored"]
+    value64f = world * cells * args.steps / (ff["ms"] * 1e-3)
+    # the ratio is quoted against the faster of the two FP64 forms (both meet the FP64
+    # bar: bit-identical, and within relative L1 1e-12, tests/test_gpu_configs.py)
+    best64 = max(value64, value64f)
     nj = sp["iters"] / args.steps
     pk, src = peaks()
     peak = float(pk["hbm_gbs"])
@@ -467,7 +478,7 @@ def main():
     # whole-step byte model for both forms (N_J = measured Jacobi sweeps per step)
     step_rf = {"unit": "GB/s", "peak": peak, "jacobi_sweeps_per_step": nj,
                "bytes_per_cell_step": {}, "achieved": {}, "frac": {}}
-    for form, val, sweeps in (("split", value, nj), ("fp64", value64, fp["iters"] / args.steps)):
+    for form, val, sweeps in (("split", value, nj), ("fp64", best64, fp["iters"] / args.steps)):
         b = STEP_BYTES_BASE[form] + STEP_BYTES_PER_SWEEP * sweeps
         step_rf["bytes_per_cell_step"][form] = b
         step_rf["achieved"][form] = val / world * b / 1e9  # per GPU (replicas)
@@ -482,9 +493,16 @@ def main():
                                f"mPDeC5, CFL 0.4, split precision, stencil Jacobi block {args.block}",
                    "cells": cells, "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
                    "l2": "inputs larger than L2 (~1.5 GB of state and stage arrays per step)"},
+        "fp64_factored": {"value": value64f, "ms_per_step": ff["ms"] / args.steps,
+                          "jacobi_iters_per_step": ff["iters"] / args.steps,
+                          "source": "per-column/row factors of the separable bathymetry "
+                                    "gradient (no per-cell table)",
+                          "rel_l1_vs_fp64_table": errors(ff["final"], fp["final"], c)["rel_l1"]},
         "fp64": {"value": value64, "ms_per_step": fp["ms"] / args.steps,
+                 "source": "bathymetry gradient tabulated at every interior Gauss point",
                  "jacobi_iters_per_step": fp["iters"] / args.steps},
-        "split_over_fp64": value / value64,
+        "split_over_fp64": value / best64,
+        "split_over_fp64_form": "fp64_factored" if value64f >= value64 else "fp64",
         "accuracy": acc,
         "accuracy_timed_steps_split_vs_fp64": short,
         "jacobi_iters_per_step": nj,

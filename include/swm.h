@@ -85,6 +85,13 @@ typedef struct swm_params {
   int mpdec2_compat;     /* 1: reproduce the hp(2,nx,ny) read of Up(:,1,:,:) of mPDeC2 and mPEuler */
   int use_graph;         /* capture each step into a CUDA graph (1 = default) */
   int device;            /* CUDA device ordinal */
+  int source_table;      /* FP64 form, Gaussian and sin/cos bathymetries: 1 (default) reads
+                          * b_x, b_y tabulated with the host libm at the 16 interior Gauss
+                          * points of every cell (256 B per cell and RHS; the reference's
+                          * source term bit for bit, equation.f90:380-388,451-509); 0 forms
+                          * the source from per-column and per-row factors of the separable
+                          * gradient (no per-cell table; equal to the reference's up to
+                          * rounding).  The split and FMA forms always use the factors. */
 } swm_params;
 
 typedef struct swm_stats {

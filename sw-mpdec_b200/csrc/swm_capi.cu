@@ -193,6 +193,8 @@ static int valid_params(const swm_params* p) {
   if (!(p->x1[0] != p->x0[0]) || !(p->x1[1] != p->x0[1]))
     return fail(SWM_ERR_PARAM, "empty domain");
   if (!(p->g > 0.0) || !(p->cfl > 0.0)) return fail(SWM_ERR_PARAM, "g and cfl must be > 0");
+  if (p->source_table != 0 && p->source_table != 1)
+    return fail(SWM_ERR_PARAM, "source_table must be 0 or 1");
   return SWM_OK;
 }
 
@@ -681,6 +683,7 @@ int swm_params_default(swm_params* p, int nx, int ny, double x00, double x01, do
   p->mpdec2_compat = 0;
   p->use_graph = 1;
   p->device = 0;
+  p->source_table = 1;
   return SWM_OK;
 }
 

@@ -81,12 +81,13 @@ inline void host_bathy_grad(const swm_params& p, double x, double y, double* bx,
   }
 }
 
-// The split and FMA forms evaluate the source of a separable gradient
-// (b_x = P(x) Q(y), b_y = R(x) T(y): the Gaussian and the sin/cos bathymetry) from
-// per-column and per-row factors; the FP64 form and the bump use the full table.
+// A separable gradient (b_x = P(x) Q(y), b_y = R(x) T(y): the Gaussian and the sin/cos
+// bathymetry) is evaluated from per-column and per-row factors, except in the FP64 form
+// with source_table = 1, which reads b_x, b_y tabulated at every interior Gauss point
+// (the reference's own products, bit for bit); the bump always takes the table.
 inline bool separable_source(const swm_params& p) {
-  return p.precision != SWM_PREC_FP64 &&
-         (p.bathy_flag == SWM_BATHY_GAUSS || p.bathy_flag == SWM_BATHY_SINCOS);
+  return (p.bathy_flag == SWM_BATHY_GAUSS || p.bathy_flag == SWM_BATHY_SINCOS) &&
+         (p.precision != SWM_PREC_FP64 || !p.source_table);
 }
 
 inline bool full_source_table(const swm_params& p) {

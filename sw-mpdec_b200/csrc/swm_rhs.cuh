@@ -611,7 +611,7 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const RhsTma* tm, con
           for (int aa = 0; aa < 4; ++aa) hq[aa][b] = (double)w[aa];
         }
       }
-      if (!done && !EX && a.src_col) {
+      if (!done && a.src_col) {
         // separable gradient: S_hu = -g sum_a Pw_a sum_b Qw_b h_ab,
         //                     S_hv = -g sum_b Tw_b sum_a Rw_a h_ab
         // 16-byte loads of the factor rows (64 bytes per column / row, 16-byte aligned)
@@ -626,19 +626,38 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const RhsTma* tm, con
           pr[2 * q + 1] = r2.y;
         }
         double s1 = 0.0, s2 = 0.0;
+        if constexpr (EX) {
+          // FP64 form: every product and sum rounded (the Gauss sums of the reference's
+          // source, equation.f90:380-388, regrouped by the separable factors)
 #pragma unroll
-        for (int aa = 0; aa < 4; ++aa) {
-          double in = 0.0;
+          for (int aa = 0; aa < 4; ++aa) {
+            double in = 0.0;
 #pragma unroll
-          for (int b = 0; b < 4; ++b) in = fma(pr[b], hq[aa][b], in);
-          s1 = fma(pc[aa], in, s1);
-        }
+            for (int b = 0; b < 4; ++b) in = __dadd_rn(in, __dmul_rn(pr[b], hq[aa][b]));
+            s1 = __dadd_rn(s1, __dmul_rn(pc[aa], in));
+          }
 #pragma unroll
-        for (int b = 0; b < 4; ++b) {
-          double in = 0.0;
+          for (int b = 0; b < 4; ++b) {
+            double in = 0.0;
 #pragma unroll
-          for (int aa = 0; aa < 4; ++aa) in = fma(pc[4 + aa], hq[aa][b], in);
-          s2 = fma(pr[4 + b], in, s2);
+            for (int aa = 0; aa < 4; ++aa) in = __dadd_rn(in, __dmul_rn(pc[4 + aa], hq[aa][b]));
+            s2 = __dadd_rn(s2, __dmul_rn(pr[4 + b], in));
+          }
+        } else {
+#pragma unroll
+          for (int aa = 0; aa < 4; ++aa) {
+            double in = 0.0;
+#pragma unroll
+            for (int b = 0; b < 4; ++b) in = fma(pr[b], hq[aa][b], in);
+            s1 = fma(pc[aa], in, s1);
+          }
+#pragma unroll
+          for (int b = 0; b < 4; ++b) {
+            double in = 0.0;
+#pragma unroll
+            for (int aa = 0; aa < 4; ++aa) in = fma(pc[4 + aa], hq[aa][b], in);
+            s2 = fma(pr[4 + b], in, s2);
+          }
         }
         S1 = -gr.g * s1;
         S2 = -gr.g * s2;

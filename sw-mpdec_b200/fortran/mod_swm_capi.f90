@@ -31,6 +31,7 @@ TYPE, BIND(C), PUBLIC :: swm_params_t
   INTEGER(C_INT)  :: well_balanced, precision, solver, jacobi_maxiter
   REAL(C_DOUBLE)  :: jacobi_tol
   INTEGER(C_INT)  :: jacobi_block, mpdec2_compat, use_graph, device
+  INTEGER(C_INT)  :: source_table
 END TYPE swm_params_t
 
 TYPE, BIND(C), PUBLIC :: swm_stats_t

@@ -51,6 +51,7 @@ class SwmParams(ctypes.Structure):
         ("jacobi_maxiter", ctypes.c_int), ("jacobi_tol", ctypes.c_double),
         ("jacobi_block", ctypes.c_int), ("mpdec2_compat", ctypes.c_int),
         ("use_graph", ctypes.c_int), ("device", ctypes.c_int),
+        ("source_table", ctypes.c_int),
     ]
 
 
@@ -141,7 +142,7 @@ def _check(rc):
 def make_params(nx, ny, x0, x1, g=9.81, cfl=1.0, timescheme=5, bathy_flag=0,
                 bathy_par=(0, 0, 0, 0, 0), well_balanced=0, precision="fp64", solver="csr",
                 jacobi_maxiter=1000, jacobi_tol=1e-16, jacobi_block=0, mpdec2_compat=0,
-                use_graph=1, device=0):
+                use_graph=1, device=0, source_table=1):
     lib = load()
     p = SwmParams()
     _check(lib.swm_params_default(ctypes.byref(p), nx, ny, x0[0], x0[1], x1[0], x1[1]))
@@ -153,6 +154,7 @@ def make_params(nx, ny, x0, x1, g=9.81, cfl=1.0, timescheme=5, bathy_flag=0,
     p.solver = SOLVER[solver] if isinstance(solver, str) else int(solver)
     p.jacobi_maxiter, p.jacobi_tol, p.jacobi_block = jacobi_maxiter, jacobi_tol, jacobi_block
     p.mpdec2_compat, p.use_graph, p.device = int(mpdec2_compat), int(use_graph), device
+    p.source_table = int(source_table)
     return p
 
 

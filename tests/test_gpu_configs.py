@@ -41,7 +41,7 @@ def report(entry):
             f.write(json.dumps(entry) + "\n")
 
 
-def setup(swm, c, precision, threaded=True):
+def setup(swm, c, precision, threaded=True, source_table=1):
     """Oracle (OpenMP build: per-cell arithmetic identical to the serial one) and a GPU
     solver on the same initial state and WB reference."""
     op = O.make_params(c["nx"], c["ny"], c["x0"], c["x1"], g=c["g"], cfl=c["cfl"],
@@ -51,7 +51,7 @@ def setup(swm, c, precision, threaded=True):
     s = swm.Solver(nx=c["nx"], ny=c["ny"], x0=c["x0"], x1=c["x1"], g=c["g"], cfl=c["cfl"],
                    bathy_flag=c["bathy_flag"], bathy_par=c["bathy_par"],
                    well_balanced=c["well_balanced"], precision=precision, solver="stencil",
-                   jacobi_block=4)
+                   jacobi_block=4, source_table=source_table)
     if c["well_balanced"]:
         wb = cases.cell_averages(c, c["wb_ic"], c["wb_par"])
         o.init_wb_planes(wb)
@@ -199,3 +199,30 @@ def test_split_mass_and_positivity_at_config_size(gpu, name, steps):
             "mass_drift_rel": drift, "min_h": hmin})
     assert hmin >= 0.0
     assert abs(drift) <= 1e-13, drift
+
+
+@pytest.mark.parametrize("name,n,xc,steps", [("island", 128, 2.0, 110), ("island", 256, 3.6, 40),
+                                             ("lake", None, None, 10),
+                                             ("lake_dry", None, None, 10)])
+def test_fp64_factored_source_within_1e12(gpu, name, n, xc, steps):
+    # the FP64 form with the bathymetry source from per-column/row factors instead of
+    # the per-cell gradient table: not bit-identical (the products are regrouped), but
+    # within the relative L1 bar of 1e-12 per variable
+    c = cases.case(name, n=n)
+    if xc is not None:
+        c["par"] = (0.3, xc, 0.3)
+    o, s = setup(gpu, c, "fp64", source_table=0)
+    t = 0.0
+    for k in range(steps):
+        dt = o.timestep()
+        o.step(t, dt)
+        assert s.step(t, dt) == 0
+        t += dt
+    ref, got = o.get_planes(), s.get_planes()
+    dx = (c["x1"][0] - c["x0"][0]) / c["nx"]
+    dy = (c["x1"][1] - c["x0"][1]) / c["ny"]
+    e = errors(got, ref, dx, dy)
+    report({"config": f"{name} {c['nx']}x{c['ny']} fp64 factored source", "steps": steps,
+            "rel_l1": e[1], "linf": e[2], "bitwise": bool(np.array_equal(got, ref))})
+    assert max(e[1]) <= 1e-12, e[1]
+    assert got[0].min() >= 0.0
