@@ -347,6 +347,7 @@ static int batch_copy_state(swm_batch* b, bool to_save) {
 // Autotuner: time one step per candidate sweeps-per-pass on the initial state,
 // restore the state after each, keep the fastest.
 static int batch_tune(swm_batch* b) {
+  NvtxRange range("ensemble autotune");
   for (auto& q : b->pr)
     for (int v = 0; v < 3; ++v)
       if (!q.save[v]) {
@@ -499,6 +500,7 @@ int swm_batch_get_planes(swm_batch_handle b, int i, double* planes) {
 }
 
 int swm_batch_step(swm_batch_handle b, double* dt_out) {
+  NvtxRange range("swm_batch_step");
   if (!b) return bfail(SWM_ERR_PARAM, "null handle");
   if (!b->have_state) return bfail(SWM_ERR_STATE, "no state set");
   BCK(cudaSetDevice(b->device));

@@ -510,9 +510,12 @@ static int enqueue_patankar(swm_solver* s) {
   const bool csr = (s->p.solver == SWM_SOLVER_CSR);
   const bool compat = two && s->p.mpdec2_compat;
   // RHS at U^n (timediscretization.f90:519), stored in slot 1 and used for all r at k=1
-  prof_mark(s, 0);
-  CK(launch_rhs(s, make_rhs_args(s, s->h, s->hu, s->hv, 0)));
-  prof_mark(s, -1);
+  {
+    NvtxRange r("rhs");
+    prof_mark(s, 0);
+    CK(launch_rhs(s, make_rhs_args(s, s->h, s->hu, s->hv, 0)));
+    prof_mark(s, -1);
+  }
   int solve = 0;
   // the three substeps of an mPDeC5 correction iteration depend only on the previous
   // iteration, so (split and FMA forms, stencil layout) they are assembled in one
@@ -561,10 +564,12 @@ static int enqueue_patankar(swm_solver* s) {
       if (fuse_k && m > 2)
         for (int c = 0; c < 5; ++c) sys[c] = s->cset[m - 3][c];
       if (!fuse_k) {
+        NvtxRange r("patankar assembly");
         prof_mark(s, 1);
         CK(launch_assemble(aa, csr, s->stream));
         prof_mark(s, -1);
       } else if (m == 2) {
+        NvtxRange r("patankar assembly (3 substeps)");
         AssembleMultiArgs ma{};
         ma.base = aa;
         ma.nm = 3;
@@ -608,13 +613,17 @@ static int enqueue_patankar(swm_solver* s) {
       ja.block = jacobi_block_of(s->p);
       ja.recip = fast_patankar(s->p) ? 1 : 0;
       ja.spin_limit = s->spin_limit;
-      prof_mark(s, 2);
-      CK(launch_jacobi(ja, csr, s->jac_blocks, s->stream));
-      prof_mark(s, -1);
+      {
+        NvtxRange r("jacobi");
+        prof_mark(s, 2);
+        CK(launch_jacobi(ja, csr, s->jac_blocks, s->stream));
+        prof_mark(s, -1);
+      }
       solve++;
     }
     if (k < kc) {  // RHS at Ua(m) (timediscretization.f90:550-557)
       for (int m = 2; m <= ms; ++m) {
+        NvtxRange r("rhs");
         prof_mark(s, 0);
         CK(launch_rhs(s, make_rhs_args(s, s->hbuf[m - 1][k & 1], s->hum[m - 1], s->hvm[m - 1],
                                        m - 1)));
@@ -628,6 +637,7 @@ static int enqueue_patankar(swm_solver* s) {
 
 static int build_graph(swm_solver* s) {
   if (s->graph || s->graph_failed || !s->p.use_graph) return SWM_OK;
+  NvtxRange range("capture step graph");
   cudaGraph_t g = nullptr;
   if (cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
     cudaGetLastError();
@@ -880,6 +890,7 @@ static int upload_ghosted(swm_solver* s, const double* U, double* h, double* hu,
 }
 
 int swm_set_state(swm_handle s, const double* U) {
+  NvtxRange range("swm_set_state");
   if (!s || !U) return fail(SWM_ERR_PARAM, "null argument");
   CK(cudaSetDevice(s->device));
   int rc = upload_ghosted(s, U, s->h, s->hu, s->hv);
@@ -890,6 +901,7 @@ int swm_set_state(swm_handle s, const double* U) {
 }
 
 int swm_get_state(swm_handle s, double* U, double* V) {
+  NvtxRange range("swm_get_state");
   if (!s || !U) return fail(SWM_ERR_PARAM, "null argument");
   if (!s->have_state) return fail(SWM_ERR_STATE, "no state set");
   CK(cudaSetDevice(s->device));
@@ -1201,6 +1213,7 @@ int swm_set_wb_state(swm_handle s, const double* Uwb) {
 }
 
 int swm_timestep(swm_handle s, double* dt_min) {
+  NvtxRange range("swm_timestep");
   if (!s || !dt_min) return fail(SWM_ERR_PARAM, "null argument");
   if (!s->have_state) return fail(SWM_ERR_STATE, "no state set");
   CK(cudaSetDevice(s->device));
@@ -1231,6 +1244,7 @@ int swm_timestep(swm_handle s, double* dt_min) {
 
 int swm_step(swm_handle s, double t, double dt) {
   (void)t;  // stage times are not read by the periodic BC or the source (equation.f90:515,284)
+  NvtxRange range("swm_step");
   if (!s) return fail(SWM_ERR_PARAM, "null handle");
   if (!s->have_state) return fail(SWM_ERR_STATE, "no state set");
   if (!(dt > 0.0) || !std::isfinite(dt)) return fail(SWM_ERR_PARAM, "dt must be finite and > 0");

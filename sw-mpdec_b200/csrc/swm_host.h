@@ -2,6 +2,8 @@
 // mesh and quadrature (mesh.f90:58-70, :127-142) and the bathymetry tables the RHS
 // kernels read.
 #pragma once
+#include <nvtx3/nvToolsExt.h>
+
 #include <cmath>
 #include <cstddef>
 #include <vector>
@@ -11,6 +13,16 @@
 #include "swm_rhs.cuh"
 
 namespace swm {
+
+// NVTX range for the lifetime of the object: the C-ABI calls and, when a step is
+// enqueued eagerly or captured, its phases show up by name in a profiler timeline
+// (no cost without an attached tool).
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // 4-point Gauss-Legendre nodes on [-1/2, 1/2] and weights (mesh.f90:127-129).
 inline void host_quadrature(double qn[4], double qw[4]) {
