@@ -140,11 +140,13 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def make_solver(swm, c, precision, solver="stencil", block=4, device=0, source_table=1):
+def make_solver(swm, c, precision, solver="stencil", block=4, device=0, source_table=1,
+                timescheme=5):
     return swm.Solver(nx=c["nx"], ny=c["ny"], x0=c["x0"], x1=c["x1"], g=c["g"], cfl=c["cfl"],
                       bathy_flag=c["bathy_flag"], bathy_par=c["bathy_par"],
                       well_balanced=c["well_balanced"], precision=precision, solver=solver,
-                      jacobi_block=block, device=device, source_table=source_table)
+                      jacobi_block=block, device=device, source_table=source_table,
+                      timescheme=timescheme)
 
 
 # Timed forms: the split form (the metric's numerator) and the plain FP64 form twice,
@@ -338,6 +340,10 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--n", type=int, default=2048)
+    # profiling runs only: a subset of the timed forms, or another time scheme (its
+    # kernels under ncu); either prints the per-form step times and nothing else
+    ap.add_argument("--forms", default=",".join(FORMS))
+    ap.add_argument("--timescheme", type=int, default=5)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -372,8 +378,12 @@ def main():
 
     results = {}
     clocks = None
-    for prec, (form, table) in FORMS.items():
-        s = make_solver(swm, c, form, block=args.block, device=local, source_table=table)
+    forms = args.forms.split(",")
+    partial = set(forms) != set(FORMS) or args.timescheme != 5
+    for prec in forms:
+        form, table = FORMS[prec]
+        s = make_solver(swm, c, form, block=args.block, device=local, source_table=table,
+                        timescheme=args.timescheme)
         s.set_planes(planes)
         barrier()
         sampler = ClockSampler(local) if prec == "split" else None
@@ -386,10 +396,24 @@ def main():
         barrier()
         ms = max_over_ranks(ms)
         prof = s.profile_step(0.0, s.timestep())  # one extra eagerly-launched step
-        results[prec] = dict(ms=ms, iters=iters, prof=prof, final=s.get_planes())
+        final = s.get_planes()
+        prof_wrapped = None
+        if prec == "split" and not partial:  # the RHS with every tile loaded without TMA
+            s.set_tma(False)
+            prof_wrapped = s.profile_step(0.0, s.timestep())
+            s.set_tma(True)
+        results[prec] = dict(ms=ms, iters=iters, prof=prof, final=final, prof_wrapped=prof_wrapped)
         s.close()
         del s
 
+    if partial:
+        if rank == 0:
+            print(json.dumps({"profiling_run": True, "timescheme": args.timescheme,
+                              "ms_per_step": {k: v["ms"] / args.steps for k, v in results.items()}}),
+                  flush=True)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
     # the split form against the FP64 form after the timed steps (short horizon); the
     # wet-dry accuracy leg against the oracle runs after the GPU legs
     short = errors(results["split"]["final"], results["fp64"]["final"], c)
@@ -543,6 +567,12 @@ def main():
         "accuracy_timed_steps_split_vs_fp64": short,
         "jacobi_iters_per_step": nj,
         "kernel_ms_per_step": {k: v[0] for k, v in classes.items()},
+        "rhs_tile_loads": {
+            "tma_us_per_launch": 1e3 * pr["rhs_ms"] / max(pr["rhs_launches"], 1),
+            "wrapped_us_per_launch": 1e3 * sp["prof_wrapped"]["rhs_ms"] /
+                                     max(sp["prof_wrapped"]["rhs_launches"], 1),
+            "note": "split RHS per launch, one eagerly launched step each: interior tiles "
+                    "staged by TMA tensor copies vs every tile by wrapped-index loads"},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                      "traffic_source": traffic_src, "alg_bytes_per_launch": alg,
