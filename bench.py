@@ -465,26 +465,39 @@ def main():
         bt = swm.Batch(plist)
         for k, i in enumerate(mine):
             bt.set_planes(k, cases.cell_averages(members[i]))
-        for _ in range(max(args.warmup, 1)):  # the first step also picks sweeps per pass
+        for _ in range(max(args.warmup, 1)):  # the first step also picks the schedule
             bt.step()
-        barrier()
         st = torch.cuda.ExternalStream(bt.stream())
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(st)
-        for _ in range(args.steps):
-            bt.step()
-        e1.record(st)
-        torch.cuda.synchronize()
-        ms_ens, cell_steps = replicas.aggregate(e0.elapsed_time(e1), bt.cells() * args.steps,
+
+        def time_ensemble():
+            barrier()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            for _ in range(args.steps):
+                bt.step()
+            e1.record(st)
+            torch.cuda.synchronize()
+            return e0.elapsed_time(e1)
+
+        ms_ens, cell_steps = replicas.aggregate(time_ensemble(), bt.cells() * args.steps,
                                                 dist, device="cuda")
         blk, tot, last = bt.stats()
+        launches, ctas = bt.launch_info()
+        # the same ensemble with one launch per phase (40 per step), for comparison
+        bt.set_launches(True)
+        for _ in range(max(args.warmup, 1)):
+            bt.step()
+        ms_phase = replicas.aggregate(time_ensemble(), 0.0, dist, device="cuda")[0]
         ens = {"workload": "256 problems, sides log-uniform in [64,512], vortex / dam break / "
                            "Gaussian lake families, seed 0, split precision",
                "value": cell_steps / (ms_ens * 1e-3), "unit": "cell-steps/s",
                "cells": int(sum(sizes)), "ms_per_step": ms_ens / args.steps,
                "jacobi_block_autotuned": blk,
                "jacobi_iters_per_step_max": int(last.sum(axis=0).max()),
-               "launches_per_step": 1 + 13 * 3}
+               "launches_per_step": launches, "persistent_ctas": ctas,
+               "per_phase_launches": {"launches_per_step": 1 + 13 * 3,
+                                      "ms_per_step": ms_phase / args.steps,
+                                      "value": cell_steps / (ms_phase * 1e-3)}}
         bt.close()
 
     if rank != 0:

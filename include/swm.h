@@ -254,13 +254,16 @@ SWM_API int swm_jacobi_noalloc(int nx, int ny, const double *cS, const double *c
 
 /* ---- batched ensembles ---- */
 typedef struct swm_batch *swm_batch_handle;
-/* n problems of independent size and parameters, stepped together: one launch
- * per phase covers every problem's tiles (the Jacobi solve is one cooperative
- * launch in which each problem keeps its own stop rule), and the whole step is a
- * CUDA graph.  All problems share precision and jacobi_block (taken from p[0]);
- * mPDeC5 only, no well-balanced reference; the stencil solver is always used.
- * jacobi_block = 0 lets the first step time 2, 4 and 8 sweeps per pass on the
- * initial state and keep the fastest. */
+/* n problems of independent size and parameters, stepped together (the
+ * reference's time loop, timediscretization.f90:57-95, over an ensemble): a whole
+ * mPDeC5 step of every problem is one cooperative persistent launch (TimeStep, the
+ * RHS of every tile, and per correction the assembly of its three substeps and one
+ * batched Jacobi solve of all their systems, each with its own stop rule), captured
+ * with its memsets as a CUDA graph.  All problems share precision and jacobi_block
+ * (taken from p[0]); mPDeC5 only, no well-balanced reference; the stencil solver is
+ * always used.  jacobi_block = 0 lets the first step time the schedules (2, 4 and 8
+ * sweeps per pass, one or two CTAs per SM) on the initial state and keep the
+ * fastest; every schedule gives the same results. */
 SWM_API int swm_batch_create(int n, const swm_params *p, swm_batch_handle *out);
 SWM_API int swm_batch_destroy(swm_batch_handle b);
 SWM_API int swm_batch_set_planes(swm_batch_handle b, int i, const double *planes);
@@ -276,6 +279,19 @@ SWM_API int swm_batch_get_stats(swm_batch_handle b, int *jacobi_block, long long
                                 int *last_iters);
 /* The cudaStream_t the ensemble launches on (for CUDA-event timing by the caller). */
 SWM_API int swm_batch_get_stream(swm_batch_handle b, void **stream);
+/* Debug/measurement: per_phase = 1 steps the ensemble with one launch per phase
+ * (40 per step: TimeStep, 13 RHS, 13 assemblies, 13 Jacobi solves, every solve in
+ * one system buffer), 0 (default) with the one persistent launch; results are
+ * identical.  Resets the captured graph. */
+SWM_API int swm_batch_debug_set_launches(swm_batch_handle b, int per_phase);
+/* Measurement: one step of every problem (it advances the state) by the persistent
+ * launch, recording when its phases end; ms[0..n-1] (cap >= 16) receive the phase
+ * durations: TimeStep, RHS of U^n, then per correction k = 1..5 the assembly, the
+ * Jacobi solve and (k < 5) the RHS of the new substeps. */
+SWM_API int swm_batch_debug_phase_times(swm_batch_handle b, double *ms, int cap, int *n);
+/* Launches of the ensemble's own kernels in one step (1 or 40) and the CTAs of the
+ * persistent launch (0 when per phase). */
+SWM_API int swm_batch_get_launch_info(swm_batch_handle b, int *launches_per_step, int *ctas);
 
 #ifdef __cplusplus
 }

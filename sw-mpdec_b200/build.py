@@ -2,8 +2,9 @@
 
 Translation units and their floating-point flags:
   swm_kernels.cu    -fmad=false  (Patankar assembly, Jacobi, dt, layouts)
-  swm_rhs_exact.cu  -fmad=false  (RHS, reference expression order)
-  swm_rhs_fast.cu   default      (RHS, FP64 with contraction and the split form)
+  swm_rhs_exact.cu  -fmad=false  (RHS, reference expression order; FP64 ensemble step)
+  swm_rhs_fast.cu   default      (RHS, FP64 with contraction and the split form;
+                                  their ensemble steps)
   swm_capi.cu       host orchestration, C ABI
   swm_batch.cu      batched ensembles
   swm_noalloc.cu    allocation-free Jacobi entry point

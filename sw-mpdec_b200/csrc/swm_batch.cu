@@ -1,12 +1,17 @@
 // swm_batch.cu -- ensembles of independent problems on uneven grids.
 //
-// Every phase of an mPDeC5 step is one launch covering all problems: the batched
-// dt reduction (per-problem TimeStep, computed on the device), 13 batched RHS
-// launches (one CTA per (problem, tile)), 13 batched assemblies and 13 cooperative
-// Jacobi launches in which each problem keeps its own stop rule.  The whole step
-// is captured once into a CUDA graph.  jacobi_block = 0 lets the first step try
-// the candidate sweeps-per-pass on the initial state and keep the fastest
-// (results do not depend on it: every candidate produces the same iterates).
+// A whole mPDeC5 step of every problem is one cooperative persistent launch (the
+// ensemble step kernel, swm_ensemble.cuh): per-problem TimeStep, the RHS of every
+// (problem, tile), and per correction the assembly of its three substeps into three
+// independent Patankar systems per problem and one batched Jacobi solve of all of
+// them, each system with its own stop rule, phases separated by bounded grid
+// barriers.  The step (three memsets and that launch) is captured once into a CUDA
+// graph.  jacobi_block = 0 lets the first step time the candidate schedules -- Jacobi
+// temporal block (sweeps per pass, which sets the haloed tile shape 64+2T x 16+2T)
+// and CTAs per SM -- on the initial state and keep the fastest (results do not depend
+// on it: every candidate produces the same iterates).  The earlier form, one launch
+// per phase (40 per step), stays selectable for comparison
+// (swm_batch_debug_set_launches).
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -45,6 +50,7 @@ const double kTh5[4][4] = {
 const int kSolves = 13;    // mPDeC5: 3 substeps x 4 corrections + 1
 const int kRhsSets = 7;    // U^n, and Ua(m) for m = 2..4 at both correction parities
 const int kCandidates[3] = {2, 4, 8};
+const int kSubsteps = 3;   // systems per problem solved together (substeps m = 2..4)
 
 struct BProblem {
   swm_params p{};
@@ -59,8 +65,12 @@ struct BProblem {
   double* fv[4] = {};
   double* fxm[4] = {};
   double* fym[4] = {};
-  double *cS = nullptr, *cW = nullptr, *cE = nullptr, *cN = nullptr, *cD = nullptr;
-  double *xa = nullptr, *xb = nullptr;
+  // Patankar systems: one per substep m = 2..4 (set q = m - 2; the single-launch-per-
+  // phase path and the last correction use set 0), planes S, W, E, N, D and the two
+  // Jacobi iterate buffers
+  double* sys[kSubsteps][5] = {};
+  double* xa[kSubsteps] = {};
+  double* xb[kSubsteps] = {};
   double *src_col = nullptr, *src_row = nullptr, *bgrad = nullptr;
   SrcSplit *src_cols = nullptr, *src_rows = nullptr;
   double* save[3] = {};  // state copy used while tuning
@@ -75,8 +85,20 @@ struct swm_batch {
   cudaStream_t stream = nullptr;
   std::vector<void*> allocs;
   RhsArgs* d_rhs = nullptr;        // [kRhsSets][n]
-  AssembleArgs* d_asm = nullptr;   // [kSolves][n]
+  AssembleArgs* d_asm = nullptr;   // [kSolves][n], every solve in system set 0
   JacobiArgs* d_jac = nullptr;     // [kSolves][n]
+  // persistent step: per-substep systems
+  AssembleArgs* d_asm3 = nullptr;        // [kSolves][n], outputs in the substep's set
+  AssembleMultiArgs* d_asmm = nullptr;   // [4][n] fused substeps of corrections 1..4
+  JacobiArgs* d_jac5 = nullptr;          // [5][kSubsteps n] systems of each correction
+  int2* d_cells256 = nullptr;            // kEnsCells-cell blocks (problem, first cell)
+  int ncell256 = 0;
+  bool persistent = true;                // one launch per step (else one per phase)
+  int ens_grid = 0;                      // CTAs of the step kernel (autotuned)
+  int ens_max[9] = {};                   // co-resident CTAs of the step kernel, per block
+  unsigned long long* d_clock = nullptr; // phase timestamps (swm_batch_debug_phase_times)
+  unsigned int* d_work = nullptr;        // work-item counters of the step kernel's phases
+  bool clocked = false;
   int4* d_rhs_work = nullptr;
   int nrhs = 0;
   int2* d_cells = nullptr;         // 128-cell blocks (problem, first cell)
@@ -151,13 +173,11 @@ static int batch_alloc_problem(swm_batch* b, BProblem& q) {
     BA(q.fxm[r], nfx);
     BA(q.fym[r], nfy);
   }
-  BA(q.cS, N);
-  BA(q.cW, N);
-  BA(q.cE, N);
-  BA(q.cN, N);
-  BA(q.cD, N);
-  BA(q.xa, N);
-  BA(q.xb, N);
+  for (int q3 = 0; q3 < kSubsteps; ++q3) {
+    for (int c = 0; c < 5; ++c) BA(q.sys[q3][c], N);
+    BA(q.xa[q3], N);
+    BA(q.xb[q3], N);
+  }
 #undef BA
   if (rc) return rc;
   const Grid& gr = q.gr;
@@ -203,12 +223,73 @@ static RhsArgs batch_rhs_desc(const BProblem& q, const double* h, const double* 
   return a;
 }
 
-// Descriptor tables of the fixed step sequence (the same sequence enqueue_step issues).
+// Assembly descriptor of solve (k, m) of problem q with its outputs in system set qs.
+static AssembleArgs batch_asm_desc(const swm_batch* b, const BProblem& q, int i, int k, int m,
+                                   int qs) {
+  const bool last = (k == 5);
+  AssembleArgs aa{};
+  aa.nx = q.nx;
+  aa.ny = q.ny;
+  aa.dx = q.gr.dx;
+  aa.dy = q.gr.dy;
+  aa.m = m;
+  aa.msteps = 4;
+  for (int r = 0; r < 4; ++r) aa.theta[r] = kTh5[m - 1][r];
+  aa.dt = b->d_dt + i;
+  aa.hu_n = q.hu;
+  aa.hv_n = q.hv;
+  for (int r = 0; r < 4; ++r) {
+    const int slot = (k == 1) ? 0 : r;
+    aa.fu[r] = q.fu[slot];
+    aa.fv[r] = q.fv[slot];
+    aa.fxm[r] = q.fxm[slot];
+    aa.fym[r] = q.fym[slot];
+    aa.hp[r] = (r == 0 || k == 1) ? q.h : q.hbuf[r][(k - 1) & 1];
+  }
+  aa.hu_out = last ? q.hu : q.hum[m - 1];
+  aa.hv_out = last ? q.hv : q.hvm[m - 1];
+  aa.cS = q.sys[qs][0];
+  aa.cW = q.sys[qs][1];
+  aa.cE = q.sys[qs][2];
+  aa.cN = q.sys[qs][3];
+  aa.cD = q.sys[qs][4];
+  aa.fast = b->fast ? 1 : 0;
+  aa.inv_dx = 1.0 / q.gr.dx;
+  aa.inv_dy = 1.0 / q.gr.dy;
+  return aa;
+}
+
+// Jacobi descriptor of solve (k, m) of problem q on system set qs.
+static JacobiArgs batch_jac_desc(const swm_batch* b, const BProblem& q, int k, int m, int qs) {
+  JacobiArgs jj{};
+  jj.nx = q.nx;
+  jj.ny = q.ny;
+  jj.maxiter = q.p.jacobi_maxiter;
+  residual_limbs_host(q.p.jacobi_tol * (double)q.N, jj.thresh);
+  jj.b = q.h;
+  jj.cS = q.sys[qs][0];
+  jj.cW = q.sys[qs][1];
+  jj.cE = q.sys[qs][2];
+  jj.cN = q.sys[qs][3];
+  jj.cD = q.sys[qs][4];
+  jj.xa = q.xa[qs];
+  jj.xb = q.xb[qs];
+  jj.out = (k == 5) ? q.h : q.hbuf[m - 1][k & 1];
+  jj.recip = b->fast ? 1 : 0;
+  return jj;
+}
+
+// Descriptor tables of the fixed step sequence (the same sequence enqueue_step issues):
+// for the one-launch-per-phase path every solve in system set 0; for the persistent
+// step each substep m of a correction in its own set m - 2 (the last correction's
+// single solve in set 0), the fused substeps of corrections 1..4 (fast forms), and
+// the Jacobi systems of each correction.
 static int batch_tables(swm_batch* b) {
   const int n = b->n;
   std::vector<RhsArgs> rhs((size_t)kRhsSets * n);
-  std::vector<AssembleArgs> as((size_t)kSolves * n);
-  std::vector<JacobiArgs> ja((size_t)kSolves * n);
+  std::vector<AssembleArgs> as((size_t)kSolves * n), as3((size_t)kSolves * n);
+  std::vector<AssembleMultiArgs> am((size_t)4 * n);
+  std::vector<JacobiArgs> ja((size_t)kSolves * n), ja5((size_t)5 * kSubsteps * n);
   for (int i = 0; i < n; ++i) {
     const BProblem& q = b->pr[i];
     rhs[i] = batch_rhs_desc(q, q.h, q.hu, q.hv, 0);
@@ -220,57 +301,38 @@ static int batch_tables(swm_batch* b) {
     for (int k = 1; k <= 5; ++k) {
       const int mlo = (k == 5) ? 4 : 2;
       for (int m = mlo; m <= 4; ++m, ++solve) {
-        const bool last = (k == 5);
-        AssembleArgs& aa = as[(size_t)solve * n + i];
-        aa.nx = q.nx;
-        aa.ny = q.ny;
-        aa.dx = q.gr.dx;
-        aa.dy = q.gr.dy;
-        aa.m = m;
-        aa.msteps = 4;
-        for (int r = 0; r < 4; ++r) aa.theta[r] = kTh5[m - 1][r];
-        aa.dt = b->d_dt + i;
-        aa.hu_n = q.hu;
-        aa.hv_n = q.hv;
-        for (int r = 0; r < 4; ++r) {
-          const int slot = (k == 1) ? 0 : r;
-          aa.fu[r] = q.fu[slot];
-          aa.fv[r] = q.fv[slot];
-          aa.fxm[r] = q.fxm[slot];
-          aa.fym[r] = q.fym[slot];
-          aa.hp[r] = (r == 0 || k == 1) ? q.h : q.hbuf[r][(k - 1) & 1];
+        const int qs = (k == 5) ? 0 : m - 2;
+        as[(size_t)solve * n + i] = batch_asm_desc(b, q, i, k, m, 0);
+        as3[(size_t)solve * n + i] = batch_asm_desc(b, q, i, k, m, qs);
+        ja[(size_t)solve * n + i] = batch_jac_desc(b, q, k, m, 0);
+        ja5[((size_t)(k - 1) * kSubsteps + qs) * n + i] = batch_jac_desc(b, q, k, m, qs);
+      }
+      if (k < 5) {  // the three substeps of this correction fused per cell
+        AssembleMultiArgs& ma = am[(size_t)(k - 1) * n + i];
+        ma.base = as3[(size_t)(solve - kSubsteps) * n + i];
+        ma.nm = kSubsteps;
+        for (int qq = 0; qq < kSubsteps; ++qq) {
+          const AssembleArgs& s3 = as3[(size_t)(solve - kSubsteps + qq) * n + i];
+          ma.m[qq] = s3.m;
+          for (int r = 0; r < 4; ++r) ma.theta[qq][r] = s3.theta[r];
+          ma.hu_out[qq] = s3.hu_out;
+          ma.hv_out[qq] = s3.hv_out;
+          ma.cS[qq] = s3.cS;
+          ma.cW[qq] = s3.cW;
+          ma.cE[qq] = s3.cE;
+          ma.cN[qq] = s3.cN;
+          ma.cD[qq] = s3.cD;
         }
-        aa.hu_out = last ? q.hu : q.hum[m - 1];
-        aa.hv_out = last ? q.hv : q.hvm[m - 1];
-        aa.cS = q.cS;
-        aa.cW = q.cW;
-        aa.cE = q.cE;
-        aa.cN = q.cN;
-        aa.cD = q.cD;
-        aa.fast = b->fast ? 1 : 0;
-        aa.inv_dx = 1.0 / q.gr.dx;
-        aa.inv_dy = 1.0 / q.gr.dy;
-        JacobiArgs& jj = ja[(size_t)solve * n + i];
-        jj.nx = q.nx;
-        jj.ny = q.ny;
-        jj.maxiter = q.p.jacobi_maxiter;
-        residual_limbs_host(q.p.jacobi_tol * (double)q.N, jj.thresh);
-        jj.b = q.h;
-        jj.cS = q.cS;
-        jj.cW = q.cW;
-        jj.cE = q.cE;
-        jj.cN = q.cN;
-        jj.cD = q.cD;
-        jj.xa = q.xa;
-        jj.xb = q.xb;
-        jj.out = last ? q.h : q.hbuf[m - 1][k & 1];
-        jj.recip = b->fast ? 1 : 0;
       }
     }
   }
   BCK(cudaMemcpy(b->d_rhs, rhs.data(), sizeof(RhsArgs) * rhs.size(), cudaMemcpyHostToDevice));
   BCK(cudaMemcpy(b->d_asm, as.data(), sizeof(AssembleArgs) * as.size(), cudaMemcpyHostToDevice));
   BCK(cudaMemcpy(b->d_jac, ja.data(), sizeof(JacobiArgs) * ja.size(), cudaMemcpyHostToDevice));
+  BCK(cudaMemcpy(b->d_asm3, as3.data(), sizeof(AssembleArgs) * as3.size(), cudaMemcpyHostToDevice));
+  BCK(cudaMemcpy(b->d_asmm, am.data(), sizeof(AssembleMultiArgs) * am.size(),
+                 cudaMemcpyHostToDevice));
+  BCK(cudaMemcpy(b->d_jac5, ja5.data(), sizeof(JacobiArgs) * ja5.size(), cudaMemcpyHostToDevice));
   return SWM_OK;
 }
 
@@ -283,7 +345,7 @@ static cudaError_t batch_rhs(swm_batch* b, int set) {
 
 // One mPDeC5 step of every problem (timediscretization.f90:458-566), dt per problem
 // from the batched TimeStep, all on b->stream.
-static int batch_enqueue(swm_batch* b, int block) {
+static int batch_enqueue_phases(swm_batch* b, int block) {
   BCK(cudaMemsetAsync(b->d_ctl, 0, sizeof(JacBatchCtl), b->stream));
   BCK(launch_dt_batch(b->d_dtd, b->d_cells, b->ncellblk, b->n, b->d_lam, b->d_bad, b->d_dt,
                       b->stream));
@@ -299,6 +361,7 @@ static int batch_enqueue(swm_batch* b, int block) {
       ja.tiles = b->d_tiles;
       ja.ntiles = b->ntiles;
       ja.nprob = b->n;
+      ja.nsets = 1;
       ja.st = b->d_st;
       ja.ctl = b->d_ctl;
       ja.iters = b->d_iters + (size_t)solve * b->n;
@@ -312,11 +375,71 @@ static int batch_enqueue(swm_batch* b, int block) {
   return SWM_OK;
 }
 
+// The ensemble step kernel of this batch's form for Jacobi temporal block tb.
+static const void* ens_kernel(const swm_batch* b, int tb) {
+  const int t = tb <= 2 ? 2 : (tb <= 4 ? 4 : 8);
+  return b->precision == SWM_PREC_FP64
+             ? ensemble_kernel_exact(t)
+             : ensemble_kernel_fast(b->precision == SWM_PREC_SPLIT ? 1 : 0, t);
+}
+
+// One mPDeC5 step of every problem in one cooperative launch of `grid` CTAs (at most
+// the co-resident count), `block` Jacobi sweeps per pass.
+static int batch_enqueue_persistent(swm_batch* b, int block, int grid) {
+  BCK(cudaMemsetAsync(b->d_lam, 0, sizeof(unsigned long long) * 2 * b->n, b->stream));
+  BCK(cudaMemsetAsync(b->d_bad, 0, sizeof(int) * b->n, b->stream));
+  BCK(cudaMemsetAsync(b->d_ctl, 0, sizeof(JacBatchCtl), b->stream));
+  BCK(cudaMemsetAsync(b->d_work, 0, sizeof(unsigned int) * kEnsCounters, b->stream));
+  EnsembleArgs a{};
+  a.nprob = b->n;
+  a.precision = b->precision;
+  a.dtd = b->d_dtd;
+  a.cells = b->d_cells256;
+  a.ncells = b->ncell256;
+  a.lam = b->d_lam;
+  a.bad = b->d_bad;
+  a.dt = b->d_dt;
+  a.rhs = b->d_rhs;
+  a.rtiles = b->d_rhs_work;
+  a.nrtiles = b->nrhs;
+  a.asmd = b->d_asm3;
+  a.asmm = b->d_asmm;
+  a.jac = b->d_jac5;
+  a.jtiles = b->d_tiles;
+  a.njtiles = b->ntiles;
+  a.st = b->d_st;
+  a.ctl = b->d_ctl;
+  a.iters = b->d_iters;
+  a.block = block;
+  a.spin_limit = kDefaultSpinLimit;
+  a.clock = b->clocked ? b->d_clock : nullptr;
+  a.work = b->d_work;
+  const int tb = block <= 2 ? 2 : (block <= 4 ? 4 : 8);
+  const int gmax = b->ens_max[tb];
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid < 1 || grid > gmax ? gmax : grid);
+  cfg.blockDim = dim3(256);
+  cfg.dynamicSmemBytes = ensemble_smem_bytes(tb, b->precision);
+  cfg.stream = b->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  void* args[] = {&a};
+  BCK(cudaLaunchKernelExC(&cfg, ens_kernel(b, tb), args));
+  return SWM_OK;
+}
+
+static int batch_enqueue(swm_batch* b, int block, int grid) {
+  return b->persistent ? batch_enqueue_persistent(b, block, grid) : batch_enqueue_phases(b, block);
+}
+
 static int batch_graph(swm_batch* b) {
   if (b->graph) return SWM_OK;
   cudaGraph_t g = nullptr;
   BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-  int rc = batch_enqueue(b, b->block);
+  int rc = batch_enqueue(b, b->block, b->ens_grid);
   cudaError_t e = cudaStreamEndCapture(b->stream, &g);
   if (rc) {
     if (g) cudaGraphDestroy(g);
@@ -344,8 +467,10 @@ static int batch_copy_state(swm_batch* b, bool to_save) {
   return SWM_OK;
 }
 
-// Autotuner: time one step per candidate sweeps-per-pass on the initial state,
-// restore the state after each, keep the fastest.
+// Autotuner: time one step per candidate schedule on the initial state, restore the
+// state after each, keep the fastest.  Candidates: Jacobi temporal block 2, 4, 8 (the
+// haloed tile of a pass is 64+2T x 16+2T cells) and, for the persistent step, the
+// co-resident grid or half of it (one CTA per SM instead of two).
 static int batch_tune(swm_batch* b) {
   NvtxRange range("ensemble autotune");
   for (auto& q : b->pr)
@@ -356,15 +481,26 @@ static int batch_tune(swm_batch* b) {
       }
   int rc = batch_copy_state(b, true);
   if (rc) return rc;
+  int sms = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
+  std::vector<std::pair<int, int>> cands;  // (block, grid)
+  for (int c : kCandidates) {
+    if (!b->persistent) {
+      cands.emplace_back(c, 0);
+      continue;
+    }
+    cands.emplace_back(c, b->ens_max[c]);
+    if (b->ens_max[c] >= 2 * sms) cands.emplace_back(c, b->ens_max[c] / 2);
+  }
   cudaEvent_t e0, e1;
   BCK(cudaEventCreate(&e0));
   BCK(cudaEventCreate(&e1));
   float best = 1e30f;
-  int best_block = 4;
-  for (int c : kCandidates) {
+  std::pair<int, int> pick = cands[0];
+  for (const auto& c : cands) {
     for (int rep = 0; rep < 2; ++rep) {  // first repetition warms the kernels
       BCK(cudaEventRecord(e0, b->stream));
-      if ((rc = batch_enqueue(b, c))) return rc;
+      if ((rc = batch_enqueue(b, c.first, c.second))) return rc;
       BCK(cudaEventRecord(e1, b->stream));
       BCK(cudaStreamSynchronize(b->stream));
       if ((rc = batch_copy_state(b, false))) return rc;
@@ -373,13 +509,14 @@ static int batch_tune(swm_batch* b) {
     BCK(cudaEventElapsedTime(&ms, e0, e1));
     if (ms < best) {
       best = ms;
-      best_block = c;
+      pick = c;
     }
   }
   BCK(cudaStreamSynchronize(b->stream));
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  b->block = best_block;
+  b->block = pick.first;
+  b->ens_grid = pick.second;
   b->autotune = false;
   return SWM_OK;
 }
@@ -425,7 +562,7 @@ int swm_batch_create(int n, const swm_params* p, swm_batch_handle* out) {
     return cleanup(bfail(SWM_ERR_CUDA, "cudaStreamCreate failed"));
   b->pr.resize(n);
   std::vector<int4> rw;
-  std::vector<int2> cb, tl;
+  std::vector<int2> cb, cb256, tl;
   std::vector<DtBatchDesc> dd(n);
   for (int i = 0; i < n; ++i) {
     BProblem& q = b->pr[i];
@@ -440,6 +577,7 @@ int swm_batch_create(int n, const swm_params* p, swm_batch_handle* out) {
       for (int tx = 0; tx < (q.nx + RHS_TX - 1) / RHS_TX; ++tx)
         rw.push_back(make_int4(i, tx * RHS_TX, ty * RHS_TY, 0));
     for (size_t c0 = 0; c0 < q.N; c0 += 128) cb.push_back(make_int2(i, (int)c0));
+    for (size_t c0 = 0; c0 < q.N; c0 += kEnsCells) cb256.push_back(make_int2(i, (int)c0));
     const int jt = ((q.nx + 63) / 64) * ((q.ny + 15) / 16);  // Jacobi tiles (64 x 16)
     for (int t = 0; t < jt; ++t) tl.push_back(make_int2(i, t));
     dd[i] = DtBatchDesc{q.nx, q.ny, gr.g, p[i].cfl, gr.dx, gr.dy, q.h, q.hu, q.hv};
@@ -447,18 +585,26 @@ int swm_batch_create(int n, const swm_params* p, swm_batch_handle* out) {
   }
   b->nrhs = (int)rw.size();
   b->ncellblk = (int)cb.size();
+  b->ncell256 = (int)cb256.size();
   b->ntiles = (int)tl.size();
   if ((rc = b->alloc(&b->d_rhs, (size_t)kRhsSets * n)) || (rc = b->alloc(&b->d_asm, (size_t)kSolves * n)) ||
       (rc = b->alloc(&b->d_jac, (size_t)kSolves * n)) || (rc = b->alloc(&b->d_rhs_work, rw.size())) ||
       (rc = b->alloc(&b->d_cells, cb.size())) || (rc = b->alloc(&b->d_tiles, tl.size())) ||
       (rc = b->alloc(&b->d_dtd, (size_t)n)) || (rc = b->alloc(&b->d_dt, (size_t)n)) ||
       (rc = b->alloc(&b->d_lam, 2 * (size_t)n)) || (rc = b->alloc(&b->d_bad, (size_t)n)) ||
-      (rc = b->alloc(&b->d_st, (size_t)n)) || (rc = b->alloc(&b->d_ctl, 1)) ||
+      (rc = b->alloc(&b->d_st, (size_t)kSubsteps * n)) || (rc = b->alloc(&b->d_ctl, 1)) ||
+      (rc = b->alloc(&b->d_asm3, (size_t)kSolves * n)) ||
+      (rc = b->alloc(&b->d_asmm, (size_t)4 * n)) ||
+      (rc = b->alloc(&b->d_jac5, (size_t)5 * kSubsteps * n)) ||
+      (rc = b->alloc(&b->d_cells256, cb256.size())) ||
+      (rc = b->alloc(&b->d_work, (size_t)kEnsCounters)) ||
       (rc = b->alloc(&b->d_iters, (size_t)kSolves * n)))
     return cleanup(rc);
   if (cudaMemcpy(b->d_rhs_work, rw.data(), sizeof(int4) * rw.size(), cudaMemcpyHostToDevice) ||
       cudaMemcpy(b->d_cells, cb.data(), sizeof(int2) * cb.size(), cudaMemcpyHostToDevice) ||
       cudaMemcpy(b->d_tiles, tl.data(), sizeof(int2) * tl.size(), cudaMemcpyHostToDevice) ||
+      cudaMemcpy(b->d_cells256, cb256.data(), sizeof(int2) * cb256.size(),
+                 cudaMemcpyHostToDevice) ||
       cudaMemcpy(b->d_dtd, dd.data(), sizeof(DtBatchDesc) * n, cudaMemcpyHostToDevice))
     return cleanup(bfail(SWM_ERR_CUDA, "table upload failed"));
   if ((rc = batch_tables(b))) return cleanup(rc);
@@ -466,6 +612,20 @@ int swm_batch_create(int n, const swm_params* p, swm_batch_handle* out) {
     b->jac_blocks[c] = jacobi_batch_grid_blocks(c, b->device, b->fast);
     if (b->jac_blocks[c] < 1) return cleanup(bfail(SWM_ERR_CUDA, "Jacobi kernel cannot be resident"));
   }
+  // co-resident CTAs of the ensemble step kernel per temporal block (cooperative launch)
+  for (int c = 2; c <= kMaxBlock; c *= 2) {
+    const void* fn = ens_kernel(b, c);
+    const size_t smem = ensemble_smem_bytes(c, b->precision);
+    int per_sm = 0, sms = 0;
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+            cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 256, smem) != cudaSuccess ||
+        per_sm < 1)
+      return cleanup(bfail(SWM_ERR_CUDA, "ensemble step kernel cannot be resident"));
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
+    b->ens_max[c] = per_sm * sms;
+  }
+  b->ens_max[1] = b->ens_max[2];
   if (b->block != 1 && b->block != 2 && b->block != 4 && b->block != 8)
     b->block = b->block < 2 ? 1 : (b->block < 4 ? 2 : (b->block < 8 ? 4 : 8));
   b->h_dt.assign(n, 0.0);
@@ -544,6 +704,49 @@ int swm_batch_get_stats(swm_batch_handle b, int* jacobi_block, long long* iters_
 int swm_batch_get_stream(swm_batch_handle b, void** stream) {
   if (!b || !stream) return bfail(SWM_ERR_PARAM, "invalid argument");
   *stream = (void*)b->stream;
+  return SWM_OK;
+}
+
+int swm_batch_debug_set_launches(swm_batch_handle b, int per_phase) {
+  if (!b) return bfail(SWM_ERR_PARAM, "null handle");
+  BCK(cudaSetDevice(b->device));
+  BCK(cudaStreamSynchronize(b->stream));
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  b->graph = nullptr;
+  b->persistent = per_phase == 0;
+  if (!b->persistent && b->block > kMaxBlock) b->block = kMaxBlock;
+  return SWM_OK;
+}
+
+int swm_batch_debug_phase_times(swm_batch_handle b, double* ms, int cap, int* n) {
+  NvtxRange range("swm_batch_debug_phase_times");
+  if (!b || !ms || cap < kEnsMarks - 1) return bfail(SWM_ERR_PARAM, "invalid argument");
+  if (!b->persistent) return bfail(SWM_ERR_STATE, "phase times need the persistent step");
+  if (!b->have_state) return bfail(SWM_ERR_STATE, "no state set");
+  BCK(cudaSetDevice(b->device));
+  int rc;
+  if (b->autotune && (rc = batch_tune(b))) return rc;
+  if (!b->d_clock && (rc = b->alloc(&b->d_clock, kEnsMarks))) return rc;
+  BCK(cudaMemsetAsync(b->d_clock, 0, sizeof(unsigned long long) * kEnsMarks, b->stream));
+  b->clocked = true;
+  rc = batch_enqueue_persistent(b, b->block, b->ens_grid);
+  b->clocked = false;
+  if (rc) return rc;
+  unsigned long long t[kEnsMarks];
+  BCK(cudaMemcpyAsync(t, b->d_clock, sizeof(t), cudaMemcpyDeviceToHost, b->stream));
+  BCK(cudaStreamSynchronize(b->stream));
+  for (int i = 0; i + 1 < kEnsMarks; ++i) ms[i] = (double)(t[i + 1] - t[i]) * 1e-6;
+  if (n) *n = kEnsMarks - 1;
+  return SWM_OK;
+}
+
+int swm_batch_get_launch_info(swm_batch_handle b, int* launches_per_step, int* ctas) {
+  if (!b) return bfail(SWM_ERR_PARAM, "null handle");
+  const int tb = b->block <= 2 ? 2 : (b->block <= 4 ? 4 : 8);
+  const int gmax = b->ens_max[tb];
+  if (launches_per_step) *launches_per_step = b->persistent ? 1 : 1 + 3 * kSolves;
+  if (ctas)
+    *ctas = !b->persistent ? 0 : (b->ens_grid < 1 || b->ens_grid > gmax ? gmax : b->ens_grid);
   return SWM_OK;
 }
 

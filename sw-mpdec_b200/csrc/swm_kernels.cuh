@@ -137,14 +137,20 @@ struct JacBatchCtl {
   int status;  // 0 ok, 1 some problem hit maxIter, -4 watchdog
 };
 struct JacobiBatchArgs {
-  const JacobiArgs* descs;  // per problem: nx, ny, b, stencil planes, xa, xb, out, thresh, maxiter
+  // per system (set q, problem p -> q * nprob + p): nx, ny, b, stencil planes, xa, xb,
+  // out, thresh, maxiter
+  const JacobiArgs* descs;
   const int2* tiles;        // (problem, tile index) of every tile of every problem
   int ntiles, nprob;
-  JacBatchState* st;        // [nprob]
+  int nsets;                // independent systems per problem solved together (>= 1)
+  JacBatchState* st;        // [nsets * nprob]
   JacBatchCtl* ctl;
-  int* iters;               // [nprob] sweeps of this solve
+  int* iters;               // [nsets * nprob] sweeps of each system's solve
   int block;
   long long spin_limit;
+  // nullable: work-item counter; when set, CTAs take a pass's tiles one at a time from
+  // it (reset to 0 before every pass) instead of striding by CTA
+  unsigned int* work;
 };
 struct DtBatchDesc {
   int nx, ny;
@@ -153,6 +159,57 @@ struct DtBatchDesc {
   const double* hu;
   const double* hv;
 };
+
+// ---- ensembles in one persistent launch per mPDeC5 step ----
+constexpr int kEnsCells = 256;  // cells of one TimeStep / assembly work item (= CTA size)
+
+struct EnsembleArgs {
+  int nprob;
+  int precision;             // SWM_PREC_*: which RHS tile function runs
+  // TimeStep (equation.f90:791-837) of every problem
+  const DtBatchDesc* dtd;
+  const int2* cells;         // (problem, first cell) of every kEnsCells-cell block
+  int ncells;
+  unsigned long long* lam;   // [2 nprob] LambdaMax bit patterns, zeroed before the launch
+  int* bad;                  // [nprob] non-finite / negative depth, zeroed before the launch
+  double* dt;                // [nprob]
+  // RHS: descriptors [set][nprob] (set 0: U^n; 1 + 3 par + m - 2: Ua(m) of correction
+  // parity par) and the (problem, i0, j0) tiles of one set
+  const RhsArgs* rhs;
+  const int4* rtiles;
+  int nrtiles;
+  // combination + assembly: per (solve, problem) [13][nprob]; the fast forms' three
+  // substeps of corrections 1..4 fused per cell [4][nprob]
+  const AssembleArgs* asmd;
+  const AssembleMultiArgs* asmm;
+  // Jacobi: the systems of correction k = 1..5, [5][3 nprob]: set q = substep m - 2
+  // (the last correction's one system is set 0)
+  const JacobiArgs* jac;
+  const int2* jtiles;        // (problem, tile) of every problem's Jacobi tiles
+  int njtiles;
+  JacBatchState* st;         // [3 nprob]
+  JacBatchCtl* ctl;          // grid barrier and status, zeroed before the launch
+  int* iters;                // [13][nprob] sweeps of every solve
+  int block;                 // Jacobi sweeps per pass
+  long long spin_limit;      // grid-barrier watchdog
+  // nullable: the global timer (ns) when CTA 0 starts and leaves each phase's
+  // closing barrier, kEnsMarks entries (measurement only)
+  unsigned long long* clock;
+  // work-item counters, zeroed before the launch: [0..4] RHS phases (U^n, k = 1..4),
+  // [5..9] assembly phases (k = 1..5), [10] the Jacobi passes
+  unsigned int* work;
+};
+constexpr int kEnsCounters = 11;
+// start, TimeStep, RHS of U^n, then per correction assembly, Jacobi and (k < 5) RHS
+constexpr int kEnsMarks = 3 + 5 * 3 - 1;
+// The ensemble step kernel (swm_ensemble.cuh) of a precision form and a Jacobi
+// temporal block tb (2, 4 or 8), as instantiated in the RHS units: split and FP64-FMA
+// forms in swm_rhs_fast.cu, the FP64 form in swm_rhs_exact.cu.
+const void* ensemble_kernel_fast(int mode, int tb);  // mode 1 split, 0 FP64-FMA
+const void* ensemble_kernel_exact(int tb);
+// dynamic shared memory of that kernel: the larger of the RHS tile's and the Jacobi
+// tile's (swm_kernels.cu)
+size_t ensemble_smem_bytes(int tb, int precision);
 
 // Host launchers (swm_kernels.cu, swm_rhs_*.cu)
 cudaError_t launch_rhs_batch_fast(int mode, const RhsArgs* descs, const int4* work, int nwork,

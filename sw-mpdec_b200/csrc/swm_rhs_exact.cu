@@ -5,8 +5,11 @@
 #define SWM_EXACT 1
 #define SWM_RHS_NS rhs_exact
 #include "swm_kernels.cuh"
+#include "swm_ensemble.cuh"
 
 namespace swm {
+
+const void* ensemble_kernel_exact(int tb) { return rhs_exact::ensemble_kernel<0>(tb); }
 
 cudaError_t launch_rhs_exact(const RhsArgs& a, const RhsTma& tm, cudaStream_t s) {
   dim3 grd((a.gr.nx + RHS_TX - 1) / RHS_TX, (a.gr.ny + RHS_TY - 1) / RHS_TY);

@@ -3,8 +3,13 @@
 #define SWM_EXACT 0
 #define SWM_RHS_NS rhs_fast
 #include "swm_kernels.cuh"
+#include "swm_ensemble.cuh"
 
 namespace swm {
+
+const void* ensemble_kernel_fast(int mode, int tb) {
+  return mode == 1 ? rhs_fast::ensemble_kernel<1>(tb) : rhs_fast::ensemble_kernel<0>(tb);
+}
 
 size_t rhs_smem_bytes(int mode) {
   return mode == 1 ? RhsSmem<float>::bytes : RhsSmem<double>::bytes;

@@ -30,7 +30,8 @@ EXPORTS = [
     "swm_jacobi_noalloc", "swm_batch_get_stats", "swm_batch_get_stream",
     "swm_fill_ic", "swm_init_wb_ic", "swm_l1_error", "swm_write_output", "swm_write_mesh",
     "swm_debug_format", "swm_debug_set_spin_limit", "swm_debug_inject_alloc_failure",
-    "swm_debug_set_tma",
+    "swm_debug_set_tma", "swm_batch_debug_set_launches", "swm_batch_get_launch_info",
+    "swm_batch_debug_phase_times",
 ]
 
 
@@ -119,6 +120,9 @@ def load():
     lib.swm_batch_get_stats.argtypes = [vp, P(ctypes.c_int), P(ctypes.c_longlong),
                                         P(ctypes.c_int)]
     lib.swm_batch_get_stream.argtypes = [vp, P(vp)]
+    lib.swm_batch_debug_set_launches.argtypes = [vp, ctypes.c_int]
+    lib.swm_batch_get_launch_info.argtypes = [vp, P(ctypes.c_int), P(ctypes.c_int)]
+    lib.swm_batch_debug_phase_times.argtypes = [vp, dp, ctypes.c_int, P(ctypes.c_int)]
     lib.swm_jacobi_noalloc.argtypes = ([ctypes.c_int, ctypes.c_int] + [vp] * 7 +
                                        [ctypes.c_int, ctypes.c_double, ctypes.c_int,
                                         P(ctypes.c_int), vp])
@@ -379,6 +383,27 @@ class Batch:
         p = ctypes.c_void_p()
         _check(self.lib.swm_batch_get_stream(self.h, ctypes.byref(p)))
         return p.value or 0
+
+    def set_launches(self, per_phase):
+        """One launch per phase (True, 40 per step) or the persistent step (False)."""
+        _check(self.lib.swm_batch_debug_set_launches(self.h, 1 if per_phase else 0))
+
+    def phase_times(self):
+        """Durations (ms) of the persistent step's phases over one step (which advances
+        the state): TimeStep, RHS of U^n, then per correction assembly, Jacobi, RHS."""
+        ms = np.zeros(32)
+        n = ctypes.c_int()
+        _check(self.lib.swm_batch_debug_phase_times(self.h, _dp(ms), 32, ctypes.byref(n)))
+        names = ["timestep", "rhs_Un"]
+        for k in range(1, 6):
+            names += [f"assemble_k{k}", f"jacobi_k{k}"] + ([f"rhs_k{k}"] if k < 5 else [])
+        return dict(zip(names, ms[: n.value].tolist()))
+
+    def launch_info(self):
+        """(kernel launches per step, CTAs of the persistent launch)."""
+        n, c = ctypes.c_int(), ctypes.c_int()
+        _check(self.lib.swm_batch_get_launch_info(self.h, ctypes.byref(n), ctypes.byref(c)))
+        return n.value, c.value
 
     def stats(self):
         """(sweeps per Jacobi pass, total sweeps, last step's sweeps [13][n])."""

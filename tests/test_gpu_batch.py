@@ -1,11 +1,14 @@
 """Ensembles (swm_batch_*): every member of a batched step is bit-identical to the
-same problem stepped alone with the same precision and solver (the batched
-kernels run the single-grid tile code per problem, dt per problem comes from the
-same formula on the device), and the autotuner's choice does not change results."""
+same problem stepped alone with the same precision and solver (the ensemble step
+kernel runs the single-grid tile, assembly and Jacobi code per problem, dt per
+problem comes from the same formula on the device), FP64 members are bit-identical
+to the oracle, the persistent step (one launch) and the one-launch-per-phase step
+agree bit for bit, and the autotuner's choice does not change results."""
 import numpy as np
 import pytest
 
 import cases
+import oracle as O
 
 pytestmark = pytest.mark.gpu
 
@@ -26,7 +29,7 @@ def params(swm, c, precision, block):
                            precision=precision, solver="stencil", jacobi_block=block)
 
 
-@pytest.mark.parametrize("precision", ["fp64", "split"])
+@pytest.mark.parametrize("precision", ["fp64", "split", "fp64_fma"])
 def test_batch_members_match_single_solvers(gpu, precision):
     swm = gpu
     ms = members()
@@ -80,3 +83,64 @@ def test_batch_rejects_mixed_precision(gpu):
     with pytest.raises(swm.SwmError) as e:
         swm.Batch(ps)
     assert e.value.code == -1
+
+
+def test_batch_is_one_launch_per_step(gpu):
+    swm = gpu
+    ms = members()[:2]
+    b = swm.Batch([params(swm, c, "split", 4) for c in ms])
+    for i, c in enumerate(ms):
+        b.set_planes(i, cases.cell_averages(c))
+    b.step()
+    launches, ctas = b.launch_info()
+    assert launches == 1 and ctas >= 148
+    b.set_launches(True)
+    assert b.launch_info() == (40, 0)
+    b.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "split"])
+def test_persistent_and_per_phase_steps_identical(gpu, precision):
+    swm = gpu
+    ms = members()
+    outs = []
+    for per_phase in (False, True):
+        b = swm.Batch([params(swm, c, precision, 4) for c in ms])
+        b.set_launches(per_phase)
+        for i, c in enumerate(ms):
+            b.set_planes(i, cases.cell_averages(c))
+        dts = [b.step()[0] for _ in range(3)]
+        outs.append(([b.get_planes(i) for i in range(len(ms))], dts, b.stats()[2]))
+        b.close()
+    for a, c in zip(outs[0][0], outs[1][0]):
+        assert np.array_equal(a, c)
+    assert all(np.array_equal(x, y) for x, y in zip(outs[0][1], outs[1][1]))
+    assert np.array_equal(outs[0][2], outs[1][2])
+
+
+def test_fp64_members_match_the_oracle(gpu):
+    # members of uneven size and family, stepped in one ensemble, against the oracle
+    swm = gpu
+    ms = [cases.case("vortex", n=48, seed=1), cases.case("dambreak", n=70),
+          cases.case("island", n=64), cases.case("lake", n=90)]
+    for c in ms:
+        c["well_balanced"] = 0
+    b = swm.Batch([params(swm, c, "fp64", 0) for c in ms])
+    oracles = []
+    for i, c in enumerate(ms):
+        P = cases.cell_averages(c)
+        b.set_planes(i, P)
+        o = O.Oracle(O.make_params(c["nx"], c["ny"], c["x0"], c["x1"], g=c["g"], cfl=c["cfl"],
+                                   bathy_flag=c["bathy_flag"], bathy_par=c["bathy_par"]))
+        o.set_planes(P)
+        oracles.append(o)
+    for step in range(4):
+        dts, rc = b.step()
+        assert rc == 0
+        for i, o in enumerate(oracles):
+            dt = o.timestep()
+            assert dt == dts[i], (step, i)
+            o.step(0.0, dt)
+    for i, o in enumerate(oracles):
+        assert np.array_equal(b.get_planes(i), o.get_planes()), i
+    b.close()
