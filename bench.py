@@ -49,7 +49,7 @@ PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
 # changed after it makes the figure stale.  Scaled by cells for other grid sizes (the
 # traffic of these kernels grows with the cell count).
 NCU_TRAFFIC_2048 = {
-    "rhs": (101276672.0 + 91489792.0, "b350e1f"),
+    "rhs": (101655552.0 + 91263232.0, "2c446c5"),
     "jacobi": (403459328.0 + 58311680.0, "77d112e"),
 }
 
@@ -59,6 +59,9 @@ NCU_TRAFFIC_2048 = {
 # too (that run is also the timed CPU baseline) and both are compared with it.
 ACC_N = 256
 ACC_T_END = 0.8
+
+# Wall-clock budget of the reference arm's timed steps (host CPU).
+REF_BUDGET_S = 150.0
 
 # Algorithmic bytes per cell-step of the whole mPDeC5 step: every phase reads its
 # inputs and writes its outputs once (halo re-reads not counted), the Patankar
@@ -303,23 +306,32 @@ def reference_arm(args, rank, world):
                       bathy_flag=c["bathy_flag"], bathy_par=c["bathy_par"])
     o = O.Oracle(p, threaded=True)
     o.set_planes(cases.cell_averages(c))
+    t_step = None
     for _ in range(warm):
+        t0 = time.perf_counter()
         o.step(0.0, o.timestep())
+        t_step = time.perf_counter() - t0
+    # a step of the 2048^2 grid takes ~14 s on 16 host threads: time at most as many
+    # steps as fit in REF_BUDGET_S, so that the arm ends within a few minutes
+    steps = args.steps
+    if t_step:
+        steps = max(1, min(args.steps, int(REF_BUDGET_S / t_step)))
     t0 = time.perf_counter()
-    for _ in range(args.steps):
+    for _ in range(steps):
         o.step(0.0, o.timestep())
     el = time.perf_counter() - t0
-    v = c["nx"] * c["ny"] * args.steps / el
+    v = c["nx"] * c["ny"] * steps / el
     cores = O.threads(True)
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "cell-steps/s",
-        "n_gpus": args.gpus, "steps": args.steps, "warmup": warm,
-        "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True, "scaling": "weak",
+        "n_gpus": args.gpus, "steps": steps, "warmup": warm,
+        "ms_per_step": 1e3 * el / steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": f"island {n}x{n} periodic (wave over dry island), mPDeC5, "
                                f"CFL 0.4", "cells": n * n, "parallelism": "host threads"},
         "cpu_baseline": {"value": v, "unit": "cell-steps/s", "cores": cores, "kind": "port",
-                         "sample": f"{args.steps} mPDeC5 steps of the island case at {n}x{n} "
+                         "sample": f"{steps} mPDeC5 steps (of {args.steps} asked, at most "
+                                   f"{REF_BUDGET_S:.0f} s of them) of the island case at {n}x{n} "
                                    f"after {warm} warm-up step(s) (at most one: a step takes "
                                    f"seconds on the CPU); the Fortran reference has no "
                                    f"compiler here, so its C restatement (oracle) is timed"},
@@ -339,6 +351,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true")  # profiling runs: no wet-dry leg
     ap.add_argument("--n", type=int, default=2048)
     # profiling runs only: a subset of the timed forms, or another time scheme (its
     # kernels under ncu); either prints the per-form step times and nothing else
@@ -483,6 +496,7 @@ def main():
                                                 dist, device="cuda")
         blk, tot, last = bt.stats()
         launches, ctas = bt.launch_info()
+        phases = bt.phase_times()  # one more step, its phases timed inside the launch
         # the same ensemble with one launch per phase (40 per step), for comparison
         bt.set_launches(True)
         for _ in range(max(args.warmup, 1)):
@@ -495,6 +509,7 @@ def main():
                "jacobi_block_autotuned": blk,
                "jacobi_iters_per_step_max": int(last.sum(axis=0).max()),
                "launches_per_step": launches, "persistent_ctas": ctas,
+               "phase_ms": {k: round(v, 4) for k, v in phases.items()},
                "per_phase_launches": {"launches_per_step": 1 + 13 * 3,
                                       "ms_per_step": ms_phase / args.steps,
                                       "value": cell_steps / (ms_phase * 1e-3)}}
@@ -509,7 +524,9 @@ def main():
     # timed CPU baseline and the accuracy reference (rank 0 only, after all timing)
     acc, cpu = None, None
     try:
-        acc, cpu = accuracy_leg(swm, cases, world == 1 and not args.no_cpu, args.block, local)
+        if not args.no_accuracy:
+            acc, cpu = accuracy_leg(swm, cases, world == 1 and not args.no_cpu, args.block,
+                                    local)
     except Exception as exc:  # a failed side leg must not hide the GPU number
         acc = {"error": str(exc)}
 
