@@ -41,12 +41,6 @@ int bfail(int code, const std::string& msg) {
       return bfail(SWM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));    \
   } while (0)
 
-// thetaDeC (timediscretization.f90:491-506), rows m = 1..4
-const double kTh5[4][4] = {
-    {0.0000000000000000000, 0.0000000000000000000, 0.0000000000000000000, 0.0000000000000000000},
-    {0.1103005664791649049, 0.1896994335208351257, -0.0339073642291439076, 0.0103005664791649201},
-    {0.0730327668541684294, 0.4505740308958107176, 0.2269672331458314485, -0.0269672331458315692},
-    {0.0833333333333333287, 0.4166666666666666852, 0.4166666666666666852, 0.0833333333333333287}};
 const int kSolves = 13;    // mPDeC5: 3 substeps x 4 corrections + 1
 const int kRhsSets = 7;    // U^n, and Ua(m) for m = 2..4 at both correction parities
 const int kCandidates[3] = {2, 4, 8};
@@ -234,7 +228,7 @@ static AssembleArgs batch_asm_desc(const swm_batch* b, const BProblem& q, int i,
   aa.dy = q.gr.dy;
   aa.m = m;
   aa.msteps = 4;
-  for (int r = 0; r < 4; ++r) aa.theta[r] = kTh5[m - 1][r];
+  for (int r = 0; r < 4; ++r) aa.theta[r] = kTheta5[m - 1][r];
   aa.dt = b->d_dt + i;
   aa.hu_n = q.hu;
   aa.hv_n = q.hv;

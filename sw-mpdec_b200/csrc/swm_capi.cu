@@ -68,12 +68,6 @@ cudaError_t lib_malloc_host(void** p, size_t bytes) {
       return fail(SWM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));     \
   } while (0)
 
-// thetaDeC (timediscretization.f90:491-506), row m, column r, row-major [m][r]
-const double kTheta5[4][4] = {
-    {0.0000000000000000000, 0.0000000000000000000, 0.0000000000000000000, 0.0000000000000000000},
-    {0.1103005664791649049, 0.1896994335208351257, -0.0339073642291439076, 0.0103005664791649201},
-    {0.0730327668541684294, 0.4505740308958107176, 0.2269672331458314485, -0.0269672331458315692},
-    {0.0833333333333333287, 0.4166666666666666852, 0.4166666666666666852, 0.0833333333333333287}};
 // mPDeC2 (timediscretization.f90:604)
 const double kTheta2[2][2] = {{0.0, 0.0}, {0.5, 0.5}};
 

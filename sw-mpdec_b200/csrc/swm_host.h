@@ -24,6 +24,13 @@ struct NvtxRange {
   NvtxRange& operator=(const NvtxRange&) = delete;
 };
 
+// thetaDeC of mPDeC5 (timediscretization.f90:491-506), row m, column r, row-major [m][r]
+inline constexpr double kTheta5[4][4] = {
+    {0.0000000000000000000, 0.0000000000000000000, 0.0000000000000000000, 0.0000000000000000000},
+    {0.1103005664791649049, 0.1896994335208351257, -0.0339073642291439076, 0.0103005664791649201},
+    {0.0730327668541684294, 0.4505740308958107176, 0.2269672331458314485, -0.0269672331458315692},
+    {0.0833333333333333287, 0.4166666666666666852, 0.4166666666666666852, 0.0833333333333333287}};
+
 // 4-point Gauss-Legendre nodes on [-1/2, 1/2] and weights (mesh.f90:127-129).
 inline void host_quadrature(double qn[4], double qw[4]) {
   qw[0] = (18. - sqrt(30.)) / 72.;
