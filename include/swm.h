@@ -289,6 +289,9 @@ SWM_API int swm_batch_debug_set_launches(swm_batch_handle b, int per_phase);
  * durations: TimeStep, RHS of U^n, then per correction k = 1..5 the assembly, the
  * Jacobi solve and (k < 5) the RHS of the new substeps. */
 SWM_API int swm_batch_debug_phase_times(swm_batch_handle b, double *ms, int cap, int *n);
+/* Debug: polls of every grid-barrier wait of the ensemble's kernels before the step
+ * gives up with SWM_ERR_WATCHDOG (default 2^26; <= 0: at once).  Resets the graph. */
+SWM_API int swm_batch_debug_set_spin_limit(swm_batch_handle b, long long limit);
 /* Launches of the ensemble's own kernels in one step (1 or 40) and the CTAs of the
  * persistent launch (0 when per phase). */
 SWM_API int swm_batch_get_launch_info(swm_batch_handle b, int *launches_per_step, int *ctas);

@@ -88,6 +88,7 @@ struct swm_batch {
   int2* d_cells256 = nullptr;            // kEnsCells-cell blocks (problem, first cell)
   int ncell256 = 0;
   bool persistent = true;                // one launch per step (else one per phase)
+  long long spin_limit = kDefaultSpinLimit;  // polls of a grid-barrier wait
   int ens_grid = 0;                      // CTAs of the step kernel (autotuned)
   int ens_max[9] = {};                   // co-resident CTAs of the step kernel, per block
   unsigned long long* d_clock = nullptr; // phase timestamps (swm_batch_debug_phase_times)
@@ -360,7 +361,7 @@ static int batch_enqueue_phases(swm_batch* b, int block) {
       ja.ctl = b->d_ctl;
       ja.iters = b->d_iters + (size_t)solve * b->n;
       ja.block = block;
-      ja.spin_limit = kDefaultSpinLimit;
+      ja.spin_limit = b->spin_limit;
       BCK(launch_jacobi_batch(ja, b->jac_blocks[block], b->fast, b->stream));
     }
     if (k < 5)
@@ -405,7 +406,7 @@ static int batch_enqueue_persistent(swm_batch* b, int block, int grid) {
   a.ctl = b->d_ctl;
   a.iters = b->d_iters;
   a.block = block;
-  a.spin_limit = kDefaultSpinLimit;
+  a.spin_limit = b->spin_limit;
   a.clock = b->clocked ? b->d_clock : nullptr;
   a.work = b->d_work;
   const int tb = block <= 2 ? 2 : (block <= 4 ? 4 : 8);
@@ -731,6 +732,16 @@ int swm_batch_debug_phase_times(swm_batch_handle b, double* ms, int cap, int* n)
   BCK(cudaStreamSynchronize(b->stream));
   for (int i = 0; i + 1 < kEnsMarks; ++i) ms[i] = (double)(t[i + 1] - t[i]) * 1e-6;
   if (n) *n = kEnsMarks - 1;
+  return SWM_OK;
+}
+
+int swm_batch_debug_set_spin_limit(swm_batch_handle b, long long limit) {
+  if (!b) return bfail(SWM_ERR_PARAM, "null handle");
+  BCK(cudaSetDevice(b->device));
+  BCK(cudaStreamSynchronize(b->stream));
+  if (b->graph) cudaGraphExecDestroy(b->graph);  // the limit is a kernel parameter
+  b->graph = nullptr;
+  b->spin_limit = limit;
   return SWM_OK;
 }
 

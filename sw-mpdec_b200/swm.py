@@ -31,7 +31,7 @@ EXPORTS = [
     "swm_fill_ic", "swm_init_wb_ic", "swm_l1_error", "swm_write_output", "swm_write_mesh",
     "swm_debug_format", "swm_debug_set_spin_limit", "swm_debug_inject_alloc_failure",
     "swm_debug_set_tma", "swm_batch_debug_set_launches", "swm_batch_get_launch_info",
-    "swm_batch_debug_phase_times",
+    "swm_batch_debug_phase_times", "swm_batch_debug_set_spin_limit",
 ]
 
 
@@ -123,6 +123,7 @@ def load():
     lib.swm_batch_debug_set_launches.argtypes = [vp, ctypes.c_int]
     lib.swm_batch_get_launch_info.argtypes = [vp, P(ctypes.c_int), P(ctypes.c_int)]
     lib.swm_batch_debug_phase_times.argtypes = [vp, dp, ctypes.c_int, P(ctypes.c_int)]
+    lib.swm_batch_debug_set_spin_limit.argtypes = [vp, ctypes.c_longlong]
     lib.swm_jacobi_noalloc.argtypes = ([ctypes.c_int, ctypes.c_int] + [vp] * 7 +
                                        [ctypes.c_int, ctypes.c_double, ctypes.c_int,
                                         P(ctypes.c_int), vp])
@@ -398,6 +399,10 @@ class Batch:
         for k in range(1, 6):
             names += [f"assemble_k{k}", f"jacobi_k{k}"] + ([f"rhs_k{k}"] if k < 5 else [])
         return dict(zip(names, ms[: n.value].tolist()))
+
+    def set_spin_limit(self, limit):
+        """Polls of each grid-barrier wait before SWM_ERR_WATCHDOG (<= 0: at once)."""
+        _check(self.lib.swm_batch_debug_set_spin_limit(self.h, int(limit)))
 
     def launch_info(self):
         """(kernel launches per step, CTAs of the persistent launch)."""

@@ -102,3 +102,38 @@ def test_step_reports_nan_born_inside_the_step(gpu):
         s.step(0.0, dt)
     assert e.value.code == NAN
     assert np.array_equal(s.get_planes(), ref, equal_nan=True)
+
+
+@pytest.mark.parametrize("per_phase", [False, True])
+def test_batch_watchdog_then_recovery(gpu, per_phase):
+    # the ensemble's barrier waits give up at once: the step reports the watchdog, and
+    # after the limit is restored the same handle steps the restored state exactly as
+    # a fresh batch does
+    from test_gpu_batch import members, params
+    ms = members()[:3]
+    P = [cases.cell_averages(c) for c in ms]
+
+    def batch():
+        b = gpu.Batch([params(gpu, c, "split", 4) for c in ms])
+        b.set_launches(per_phase)
+        for i in range(len(ms)):
+            b.set_planes(i, P[i])
+        return b
+
+    b = batch()
+    b.set_spin_limit(0)
+    with pytest.raises(gpu.SwmError) as e:
+        b.step()
+    assert e.value.code == WATCHDOG
+    b.set_spin_limit(1 << 26)
+    for i in range(len(ms)):
+        b.set_planes(i, P[i])
+    dts, rc = b.step()
+    assert rc == 0
+    ref = batch()
+    dts_ref, _ = ref.step()
+    assert np.array_equal(dts, dts_ref)
+    for i in range(len(ms)):
+        assert np.array_equal(b.get_planes(i), ref.get_planes(i)), i
+    b.close()
+    ref.close()
