@@ -15,8 +15,9 @@ pytestmark = pytest.mark.gpu
 
 def members():
     out = []
-    for name, n in (("vortex", 40), ("dambreak", 56), ("lake", 72), ("island", 50),
-                    ("lake_dry", 40)):
+    # uneven sizes, odd row pitches among them (their Jacobi tiles take the 8-byte path)
+    for name, n in (("vortex", 40), ("dambreak", 57), ("lake", 73), ("island", 50),
+                    ("lake_dry", 41)):
         c = cases.case(name, n=n)
         c["well_balanced"] = 0
         out.append(c)

@@ -2,7 +2,7 @@
 oracle finishes in seconds, through the C ABI.
 
 For every configuration the plain FP64 form must be bit-identical to the oracle
-(the north-star bar is relative L1 <= 1e-12 per variable).  The split form is
+(the FP64 bar is relative L1 <= 1e-12 per variable).  The split form is
 measured against the same oracle run with the reference's error definition
 (postprocessing.f90:47,51: L1 = sum |U - U_ref| dx dy), the relative L1 and
 L-infinity per variable.
