@@ -252,6 +252,14 @@ SWM_API int swm_jacobi_noalloc(int nx, int ny, const double *cS, const double *c
                                const double *rhs, double *sol, int maxiter, double tol,
                                int block, int *iters, void *stream);
 
+/* Checked build only (libswm_checked.so, -DSWM_CHECKED): the device-side index checks
+ * at the kernels' wrapped-index sites record a failure instead of touching memory out
+ * of range.  Returns, and clears, the site of the first failing check (0 none; 1 RHS
+ * tile load, 2/3 Jacobi tile loads, 4 CSR columns, 5 mPDeC2 compatibility read, 6
+ * ensemble work item) and the number of failing checks; SWM_ERR_UNSUPPORTED in the
+ * normal build. */
+SWM_API int swm_debug_checked_status(int *site, unsigned long long *count);
+
 /* ---- batched ensembles ---- */
 typedef struct swm_batch *swm_batch_handle;
 /* n problems of independent size and parameters, stepped together (the

@@ -10,7 +10,8 @@ Translation units and their floating-point flags:
   swm_noalloc.cu    allocation-free Jacobi entry point
   swm_ic.cu         -fmad=false  (initial conditions, L1 error)
   swm_output.cu     -fmad=false  (formatted solution files)
-Usage: python sw-mpdec_b200/build.py [--verbose] [--force]
+Usage: python sw-mpdec_b200/build.py [--verbose] [--force] [--ptxas] [--checked]
+(--checked: libswm_checked.so with device-side index checks, for tests)
 """
 import os
 import subprocess
@@ -20,6 +21,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libswm.so")
+# the checked build: device-side index checks at the wrapped-index sites (SWM_IN_RANGE),
+# failures recorded instead of faulting; for tests, never loaded by the product path
+BUILD_CHECKED = os.path.join(HERE, "_build_checked")
+LIB_CHECKED = os.path.join(HERE, "libswm_checked.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
@@ -48,32 +53,33 @@ def _stale(target, deps):
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 
-def build(verbose=False, force=False, ptxas_verbose=False):
-    os.makedirs(BUILD, exist_ok=True)
+def build(verbose=False, force=False, ptxas_verbose=False, checked=False):
+    bdir, lib = (BUILD_CHECKED, LIB_CHECKED) if checked else (BUILD, LIB)
+    extra = ["-DSWM_CHECKED"] if checked else []
+    os.makedirs(bdir, exist_ok=True)
     objs = []
     hdrs = _headers()
     for src, flags in UNITS:
         s = os.path.join(CSRC, src)
         if not os.path.exists(s):
             continue
-        o = os.path.join(BUILD, src.replace(".cu", ".o"))
+        o = os.path.join(bdir, src.replace(".cu", ".o"))
         objs.append(o)
         if force or _stale(o, [s] + hdrs):
-            cmd = [NVCC, *ARCH, *COMMON, *flags, "-c", s, "-o", o]
+            cmd = [NVCC, *ARCH, *COMMON, *extra, *flags, "-c", s, "-o", o]
             if ptxas_verbose:
                 cmd += ["-Xptxas", "-v"]
             if verbose:
                 print(" ".join(cmd), flush=True)
             subprocess.run(cmd, check=True)
-    if force or _stale(LIB, objs):
-        cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-Xcompiler", "-fPIC"]
+    if force or _stale(lib, objs):
+        cmd = [NVCC, *ARCH, "-shared", "-o", lib, *objs, "-Xcompiler", "-fPIC"]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
-    return LIB
+    return lib
 
 
 if __name__ == "__main__":
-    build(verbose="--verbose" in sys.argv, force="--force" in sys.argv,
-          ptxas_verbose="--ptxas" in sys.argv)
-    print(LIB)
+    print(build(verbose="--verbose" in sys.argv, force="--force" in sys.argv,
+                ptxas_verbose="--ptxas" in sys.argv, checked="--checked" in sys.argv))

@@ -1528,6 +1528,19 @@ int swm_debug_jacobi(swm_handle s, const double* mass, const double* diag, const
   return c.status == 1 ? SWM_WARN_JACOBI_MAXITER : SWM_OK;
 }
 
+int swm_debug_checked_status(int* site, unsigned long long* count) {
+  if (!site || !count) return fail(SWM_ERR_PARAM, "null argument");
+  int sites[3] = {0, 0, 0};
+  unsigned long long counts[3] = {0, 0, 0};
+  if (check_record_kernels(&sites[0], &counts[0]) || check_record_rhs_fast(&sites[1], &counts[1]) ||
+      check_record_rhs_exact(&sites[2], &counts[2]))
+    return fail(SWM_ERR_CUDA, "reading the checked-build records failed");
+  if (sites[0] < 0) return fail(SWM_ERR_UNSUPPORTED, "not a checked build (-DSWM_CHECKED)");
+  *site = sites[0] ? sites[0] : (sites[1] ? sites[1] : sites[2]);
+  *count = counts[0] + counts[1] + counts[2];
+  return SWM_OK;
+}
+
 int swm_debug_set_tma(swm_handle s, int enable) {
   if (!s) return fail(SWM_ERR_PARAM, "null handle");
   s->tma = enable != 0;

@@ -51,6 +51,48 @@ __device__ __forceinline__ int wrap(int i, int n) {
   int r = i % n;
   return r < 0 ? r + n : r;
 }
+
+// Checked build (-DSWM_CHECKED): the wrapped-index sites of the kernels (tile and halo
+// loads of the RHS and the Jacobi, CSR column reads, the mPDeC2 compatibility read,
+// ensemble work items) check their index against the array's extent; a failing check
+// records its site (the first one, and a count) and the access is skipped, so that a
+// wrong index shows up as a status instead of a memory fault.  Without the flag the
+// checks compile to nothing.
+enum {
+  kChkRhsLoad = 1, kChkJacPairs, kChkJacCells, kChkCsr, kChkCompat2, kChkEnsItem
+};
+#ifdef SWM_CHECKED
+// one record per translation unit (each unit's device code is a module of its own)
+static __device__ int g_swm_check_site;
+static __device__ unsigned long long g_swm_check_count;
+__device__ __forceinline__ bool swm_in_range(long long i, long long n, int site) {
+  if (i >= 0 && i < n) return true;
+  atomicCAS(&g_swm_check_site, 0, site);
+  atomicAdd(&g_swm_check_count, 1ull);
+  return false;
+}
+#define SWM_IN_RANGE(i, n, site) ::swm::swm_in_range((long long)(i), (long long)(n), (site))
+// Host reader of this unit's record, read and cleared: site of the first failing check
+// (0 none) and the number of failing checks.
+#define SWM_CHECK_READER(fn)                                                             \
+  int fn(int* site, unsigned long long* count) {                                       \
+    int zero = 0;                                                                      \
+    unsigned long long zc = 0;                                                         \
+    cudaError_t e = cudaMemcpyFromSymbol(site, g_swm_check_site, sizeof(int));         \
+    if (e == cudaSuccess) e = cudaMemcpyFromSymbol(count, g_swm_check_count, sizeof(zc)); \
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_swm_check_site, &zero, sizeof(int)); \
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_swm_check_count, &zc, sizeof(zc));  \
+    return e == cudaSuccess ? 0 : -1;                                                  \
+  }
+#else
+#define SWM_IN_RANGE(i, n, site) true
+#define SWM_CHECK_READER(fn)                        \
+  int fn(int* site, unsigned long long* count) {  \
+    *site = -1;                                     \
+    *count = 0;                                     \
+    return 0;                                       \
+  }
+#endif
 __device__ __forceinline__ double dmax(double a, double b) { return (a > b) ? a : b; }
 __device__ __forceinline__ double dmin(double a, double b) { return (a < b) ? a : b; }
 

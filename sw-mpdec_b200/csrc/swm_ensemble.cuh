@@ -84,6 +84,12 @@ __device__ __forceinline__ void ens_rhs(const EnsembleArgs& a, int set0, int nse
   for (int w = s_next; w < total; w = s_next) {
     const int set = w / a.nrtiles;
     const int4 t = a.rtiles[w - set * a.nrtiles];
+    if (!SWM_IN_RANGE(t.x, a.nprob, kChkEnsItem)) {
+      __syncthreads();
+      if (threadIdx.x == 0) s_next = atomicAdd(ctr, 1u);
+      __syncthreads();
+      continue;
+    }
     if (threadIdx.x < sizeof(RhsArgs) / 8)
       reinterpret_cast<unsigned long long*>(&sr)[threadIdx.x] = reinterpret_cast<
           const unsigned long long*>(&a.rhs[(size_t)(set0 + set) * a.nprob + t.x])[threadIdx.x];

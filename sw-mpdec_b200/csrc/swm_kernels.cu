@@ -14,6 +14,8 @@
 
 namespace swm {
 
+SWM_CHECK_READER(check_record_kernels)
+
 void residual_limbs_host(double v, unsigned long long out[3]) {
   unsigned long long a, b, c;
   residual_limbs(v, a, b, c);
@@ -287,7 +289,8 @@ __device__ void csr_pass(const JacobiArgs& a, const double* xin, double* xout, b
     for (int row = (int)base + threadIdx.x; row < end; row += stride) {
       double prod = 0.;
       for (int sp = a.rowstart[row]; sp <= a.rowstart[row + 1] - 1; ++sp)
-        prod = __dadd_rn(prod, __dmul_rn(a.mass[sp - 1], __ldcg(&xin[a.cols[sp - 1] - 1])));
+        if (SWM_IN_RANGE(sp - 1, 5LL * n, kChkCsr) && SWM_IN_RANGE(a.cols[sp - 1] - 1, n, kChkCsr))
+          prod = __dadd_rn(prod, __dmul_rn(a.mass[sp - 1], __ldcg(&xin[a.cols[sp - 1] - 1])));
       const double xv = __ddiv_rn(__dsub_rn(a.b[row], prod), a.diag[row]);
       xout[row] = xv;
       acc_put<1>(acc, fabs(__dsub_rn(xv, __ldcg(&xin[row]))));

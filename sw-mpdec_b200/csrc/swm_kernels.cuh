@@ -211,6 +211,12 @@ const void* ensemble_kernel_exact(int tb);
 // tile's (swm_kernels.cu)
 size_t ensemble_smem_bytes(int tb, int precision);
 
+// Checked-build records of the three units with device-side index checks (see
+// SWM_IN_RANGE): read and cleared; site -1 when the unit was built without them.
+int check_record_kernels(int* site, unsigned long long* count);
+int check_record_rhs_fast(int* site, unsigned long long* count);
+int check_record_rhs_exact(int* site, unsigned long long* count);
+
 // Host launchers (swm_kernels.cu, swm_rhs_*.cu)
 cudaError_t launch_rhs_batch_fast(int mode, const RhsArgs* descs, const int4* work, int nwork,
                                   cudaStream_t s);

@@ -240,9 +240,13 @@ __device__ __forceinline__ void rhs_tile(const RhsArgs& a, const RhsTma* tm, con
           gj = wrap(gj, ny);
         }
         const size_t k = (size_t)gj * nx + gi;
-        lh[q] = a.h[k];
-        lhu[q] = a.hu[k];
-        lhv[q] = a.hv[k];
+        if (SWM_IN_RANGE(gi, nx, kChkRhsLoad) && SWM_IN_RANGE(gj, ny, kChkRhsLoad)) {
+          lh[q] = a.h[k];
+          lhu[q] = a.hu[k];
+          lhv[q] = a.hv[k];
+        } else {
+          lh[q] = lhu[q] = lhv[q] = 0.0;
+        }
       }
     }
   }

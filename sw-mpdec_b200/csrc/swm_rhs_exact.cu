@@ -9,6 +9,8 @@
 
 namespace swm {
 
+SWM_CHECK_READER(check_record_rhs_exact)
+
 const void* ensemble_kernel_exact(int tb) { return rhs_exact::ensemble_kernel<0>(tb); }
 
 cudaError_t launch_rhs_exact(const RhsArgs& a, const RhsTma& tm, cudaStream_t s) {

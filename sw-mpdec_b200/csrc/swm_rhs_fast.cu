@@ -7,6 +7,8 @@
 
 namespace swm {
 
+SWM_CHECK_READER(check_record_rhs_fast)
+
 const void* ensemble_kernel_fast(int mode, int tb) {
   return mode == 1 ? rhs_fast::ensemble_kernel<1>(tb) : rhs_fast::ensemble_kernel<0>(tb);
 }

@@ -126,6 +126,7 @@ __device__ __forceinline__ double hp_read(const AssembleArgs& a, int m, int i, i
     long long c = L / 4;
     int ic = (int)(c % a.nx), jc = (int)(c / a.nx);
     if (s >= 2) return 0.0;  // Up(3:4,...) are never written by mPDeC2
+    if (!SWM_IN_RANGE(jc, a.ny, kChkCompat2)) return 0.0;
     return a.hp[s][(size_t)jc * a.nx + ic];
   }
   return a.hp[m][(size_t)j * a.nx + i];
@@ -571,8 +572,11 @@ __device__ void stencil_tiles(const JacobiArgs& a, const double* xin, double* xo
         const size_t row = (size_t)gj * nx;
         for (int lp = lane; lp < HX / 2; lp += 32) {
           const int lx = 2 * lp;
-          const size_t g = row + wrap_near(i0 - TB + lx, nx);
+          const int gi = wrap_near(i0 - TB + lx, nx);
+          const size_t g = row + gi;
           const int c = ly * HX + lx;
+          if (!SWM_IN_RANGE(gi, nx - 1, kChkJacPairs) || !SWM_IN_RANGE(gj, ny, kChkJacPairs))
+            continue;
           cp_async16(&sS[c], &a.cS[g]);
           cp_async16(&sW[c], &a.cW[g]);
           cp_async16(&sE[c], &a.cE[g]);
@@ -593,6 +597,7 @@ __device__ void stencil_tiles(const JacobiArgs& a, const double* xin, double* xo
           gi = small ? wrap(gi, nx) : wrap_near(gi, nx);
           const size_t g = row + gi;
           const int c = ly * HX + lx;
+          if (!SWM_IN_RANGE(gi, nx, kChkJacCells) || !SWM_IN_RANGE(gj, ny, kChkJacCells)) continue;
           // the system is read-only during the solve: 8-byte asynchronous copies;
           // the iterate, which other CTAs wrote, by a load that bypasses L1
           cp_async8(&sS[c], &a.cS[g]);

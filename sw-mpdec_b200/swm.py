@@ -32,6 +32,7 @@ EXPORTS = [
     "swm_debug_format", "swm_debug_set_spin_limit", "swm_debug_inject_alloc_failure",
     "swm_debug_set_tma", "swm_batch_debug_set_launches", "swm_batch_get_launch_info",
     "swm_batch_debug_phase_times", "swm_batch_debug_set_spin_limit",
+    "swm_debug_checked_status",
 ]
 
 
@@ -124,6 +125,7 @@ def load():
     lib.swm_batch_get_launch_info.argtypes = [vp, P(ctypes.c_int), P(ctypes.c_int)]
     lib.swm_batch_debug_phase_times.argtypes = [vp, dp, ctypes.c_int, P(ctypes.c_int)]
     lib.swm_batch_debug_set_spin_limit.argtypes = [vp, ctypes.c_longlong]
+    lib.swm_debug_checked_status.argtypes = [P(ctypes.c_int), P(ctypes.c_ulonglong)]
     lib.swm_jacobi_noalloc.argtypes = ([ctypes.c_int, ctypes.c_int] + [vp] * 7 +
                                        [ctypes.c_int, ctypes.c_double, ctypes.c_int,
                                         P(ctypes.c_int), vp])
@@ -319,6 +321,15 @@ class Solver:
         rc = _check(self.lib.swm_debug_jacobi(self.h, _dp(mass), _dp(diag), _dp(rhs), _dp(sol),
                                               ctypes.byref(it)))
         return sol, it.value, rc
+
+
+def checked_status():
+    """(site, count) of the checked build's failing index checks, cleared; raises
+    SwmError(SWM_ERR_UNSUPPORTED) in the normal build."""
+    lib = load()
+    site, count = ctypes.c_int(), ctypes.c_ulonglong()
+    _check(lib.swm_debug_checked_status(ctypes.byref(site), ctypes.byref(count)))
+    return site.value, count.value
 
 
 def inject_alloc_failure(nth):

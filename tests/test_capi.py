@@ -88,3 +88,11 @@ def test_fortran_module_binds_every_entry_point():
             "swm_set_wb_state", "swm_timestep", "swm_step", "swm_get_stats", "swm_last_error"}
     assert core <= bound
     assert bound <= set(declared())
+
+
+def test_normal_build_has_no_checked_records():
+    # the index checks exist only in libswm_checked.so; the product library says so
+    # without touching a GPU
+    with pytest.raises(swm.SwmError) as e:
+        swm.checked_status()
+    assert e.value.code == -7
