@@ -61,10 +61,14 @@ struct BProblem {
   double* fym[4] = {};
   // Patankar systems: one per substep m = 2..4 (set q = m - 2; the single-launch-per-
   // phase path and the last correction use set 0), planes S, W, E, N, D and the two
-  // Jacobi iterate buffers
+  // Jacobi iterate buffers, rows padded to the even pitch jp (16-byte aligned rows for
+  // the Jacobi tile copies); for odd nx also the rhs h^n in that layout (bp, written
+  // by the step's first assembly)
+  int jp = 0;
   double* sys[kSubsteps][5] = {};
   double* xa[kSubsteps] = {};
   double* xb[kSubsteps] = {};
+  double* bp = nullptr;
   double *src_col = nullptr, *src_row = nullptr, *bgrad = nullptr;
   SrcSplit *src_cols = nullptr, *src_rows = nullptr;
   double* save[3] = {};  // state copy used while tuning
@@ -168,11 +172,13 @@ static int batch_alloc_problem(swm_batch* b, BProblem& q) {
     BA(q.fxm[r], nfx);
     BA(q.fym[r], nfy);
   }
+  const size_t NP = (size_t)q.jp * q.ny;
   for (int q3 = 0; q3 < kSubsteps; ++q3) {
-    for (int c = 0; c < 5; ++c) BA(q.sys[q3][c], N);
-    BA(q.xa[q3], N);
-    BA(q.xb[q3], N);
+    for (int c = 0; c < 5; ++c) BA(q.sys[q3][c], NP);
+    BA(q.xa[q3], NP);
+    BA(q.xb[q3], NP);
   }
+  if (q.jp != q.nx) BA(q.bp, NP);
 #undef BA
   if (rc) return rc;
   const Grid& gr = q.gr;
@@ -248,6 +254,8 @@ static AssembleArgs batch_asm_desc(const swm_batch* b, const BProblem& q, int i,
   aa.cE = q.sys[qs][2];
   aa.cN = q.sys[qs][3];
   aa.cD = q.sys[qs][4];
+  aa.jpitch = q.jp;
+  aa.rhs_out = (k == 1 && m == 2) ? q.bp : nullptr;  // padded rhs, once per step
   aa.fast = b->fast ? 1 : 0;
   aa.inv_dx = 1.0 / q.gr.dx;
   aa.inv_dy = 1.0 / q.gr.dy;
@@ -261,7 +269,8 @@ static JacobiArgs batch_jac_desc(const swm_batch* b, const BProblem& q, int k, i
   jj.ny = q.ny;
   jj.maxiter = q.p.jacobi_maxiter;
   residual_limbs_host(q.p.jacobi_tol * (double)q.N, jj.thresh);
-  jj.b = q.h;
+  jj.b = q.bp ? q.bp : q.h;
+  jj.pitch = q.jp;
   jj.cS = q.sys[qs][0];
   jj.cW = q.sys[qs][1];
   jj.cE = q.sys[qs][2];
@@ -565,6 +574,7 @@ int swm_batch_create(int n, const swm_params* p, swm_batch_handle* out) {
     q.nx = p[i].nx;
     q.ny = p[i].ny;
     q.N = (size_t)q.nx * q.ny;
+    q.jp = q.nx + (q.nx & 1);
     q.gr = host_grid(p[i]);
     const Grid& gr = q.gr;
     if ((rc = batch_alloc_problem(b, q))) return cleanup(rc);

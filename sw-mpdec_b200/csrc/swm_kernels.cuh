@@ -34,6 +34,7 @@ struct AssembleArgs {
   int m;                  // substep 2..4 (1-based, as in the reference)
   int msteps;             // 4 (mPDeC5) or 2 (mPDeC2)
   int compat2;            // mPDeC2 sequence-association read of hp
+  int jpitch;             // row pitch of the stencil planes and rhs_out (<= 0: nx)
   double theta[4];        // thetaDeC(m, 1:4)
   const double* dt;       // device scalar
   const double* hu_n;     // Ua(1, 2:3) = U^n momentum
@@ -83,6 +84,8 @@ struct JacobiArgs {
   int nx, ny;
   int solve_idx;          // slot in ctl->iters
   int maxiter;
+  int pitch;              // stencil: row pitch of b, the coefficient planes and xa/xb
+                          // (<= 0: nx); out is unpadded
   unsigned long long thresh[3];  // tol * n in residual units (limbs)
   const double* b;        // rhs (= hp(1) = h^n)
   // stencil coefficients

@@ -190,6 +190,7 @@ __device__ __forceinline__ void assemble_stage(const AssembleArgs& a, bool csr, 
                                                const double (&hL)[4], const double* theta,
                                                const StageOut& o) {
   const size_t k = (size_t)j * a.nx + i;
+  const size_t kj = a.jpitch > 0 ? (size_t)j * a.jpitch + i : k;  // stencil planes
   const double dt = c.dt;
   double M[4] = {0., 0., 0., 0.};
   double D = 1.;
@@ -281,17 +282,17 @@ __device__ __forceinline__ void assemble_stage(const AssembleArgs& a, bool csr, 
     // the fast stencil solver iterates x = b/D - sum (M/D) x: the row divided by its
     // Diagonal, the rhs b = hp(1,.) (timediscretization.f90:887) in the D plane
     const double rD = rcp_fast(D);
-    o.cS[k] = M[0] * rD;
-    o.cW[k] = M[1] * rD;
-    o.cE[k] = M[2] * rD;
-    o.cN[k] = M[3] * rD;
-    o.cD[k] = c.b * rD;
+    o.cS[kj] = M[0] * rD;
+    o.cW[kj] = M[1] * rD;
+    o.cE[kj] = M[2] * rD;
+    o.cN[kj] = M[3] * rD;
+    o.cD[kj] = c.b * rD;
   } else {
-    o.cS[k] = M[0];
-    o.cW[k] = M[1];
-    o.cE[k] = M[2];
-    o.cN[k] = M[3];
-    o.cD[k] = D;
+    o.cS[kj] = M[0];
+    o.cW[kj] = M[1];
+    o.cE[kj] = M[2];
+    o.cN[kj] = M[3];
+    o.cD[kj] = D;
   }
 }
 
@@ -308,7 +309,10 @@ __device__ __forceinline__ void assemble_cell(const AssembleArgs& a, bool csr, c
   load_hp(a, a.m, i, j, hK, hL);
   const StageOut o{a.hu_out, a.hv_out, a.cS, a.cW, a.cE, a.cN, a.cD};
   assemble_stage<FAST, MS>(a, csr, i, j, c, hK, hL, a.theta, o);
-  if (a.rhs_out) a.rhs_out[k] = hp_read(a, 0, i, j);  // rhs = hp(1,.) (timediscretization.f90:887)
+  if (a.rhs_out) {  // rhs = hp(1,.) (timediscretization.f90:887), in the planes' layout
+    const size_t kj = a.jpitch > 0 ? (size_t)j * a.jpitch + i : k;
+    a.rhs_out[kj] = hp_read(a, 0, i, j);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -359,14 +363,15 @@ struct JTile {
   static constexpr size_t bytes = sizeof(double) * 8 * HN;
 };
 
-// 16-byte asynchronous global->shared copy through L2 (cp.async.cg); the x iterate
-// of the previous pass was written by other CTAs, so it must not come from L1.
+// Asynchronous global->shared copies.  Both are weak reads in the memory model: a copy
+// issued after a grid barrier (fence + atomics + bar.sync) observes every write made
+// before it, such as the previous pass's iterate written by other CTAs.
+// 16 bytes through L2 (cp.async.cg, the only form of that size that skips L1).
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
   unsigned s = (unsigned)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
 }
-// 8-byte asynchronous global->shared copy through L1 (cp.async.ca), for arrays that
-// no CTA writes during the launch.
+// 8 bytes (cp.async.ca).
 __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
   unsigned s = (unsigned)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem));
@@ -435,11 +440,15 @@ __device__ __forceinline__ int wrap_near(int g, int n) {
 // sweep reads them (sweep T+1 reads columns T..HX-1-T only), and their neighbour
 // loads stay inside the tile arrays since rows 0 and HY-1 are never swept.
 // Residuals count the tile's own cells: (lx - TB, ly - TB) < (cx_lim, cy_lim).
+// PART (a tile cut by the grid's edge, cx_lim < JBX or cy_lim < JBY): the units cover
+// only the (cx_lim + 2 TB) x (cy_lim + 2 TB) box such a tile loads, so its cost
+// follows its size; the same argument bounds its reads (the pair reaching one column
+// past the region reads at most one unloaded column, and no later sweep reads it).
 __device__ __forceinline__ double2 lds2(const double* p) {
   return *reinterpret_cast<const double2*>(p);
 }
 
-template <int TB, int T, bool RECIP>
+template <int TB, int T, bool RECIP, bool PART>
 __device__ __forceinline__ void tile_sweep(const double* sm, const double* xp, double* xn,
                                            int cx_lim, int cy_lim, Acc& acc) {
   using G = JTile<TB>;
@@ -447,11 +456,28 @@ __device__ __forceinline__ void tile_sweep(const double* sm, const double* xp, d
   constexpr int P0 = T / 2, NP = (HX - T - 1) / 2 - P0 + 1;  // pairs covering [T, HX-T)
   constexpr int NU = NP * (G::HY - 2 * T), NQ = (NU + JNT - 1) / JNT;
   static_assert(HX % 2 == 0 && HN % 2 == 0, "16-byte pairs");
+  // PART: np >= 1 pairs per row, nu units; u / np = (u * mul) >> 32 with
+  // mul = floor(2^32 / np) + 1 (33 bits for np = 1), exact for u * np < 2^32
+  int np = NP, nu = NU;
+  unsigned long long mul = 0;
+  if constexpr (PART) {
+    np = (cx_lim + 2 * TB - T - 1) / 2 - P0 + 1;
+    nu = np * (cy_lim + 2 * TB - 2 * T);
+    mul = (1ull << 32) / (unsigned)np + 1ull;
+  }
 #pragma unroll
   for (int q = 0; q < NQ; ++q) {
     const int u = threadIdx.x + q * JNT;
-    if (NU % JNT != 0 && u >= NU) break;
-    const int ly = T + u / NP, lx = 2 * (P0 + u % NP);
+    if (PART ? u >= nu : (NU % JNT != 0 && u >= NU)) break;
+    int row, pr;
+    if constexpr (PART) {
+      row = (int)(((unsigned long long)u * mul) >> 32);
+      pr = u - row * np;
+    } else {
+      row = u / NP;
+      pr = u % NP;
+    }
+    const int ly = T + row, lx = 2 * (P0 + pr);
     const int c = ly * HX + lx;
     // RECIP (split form): the planes hold the row divided by its Diagonal and b/D
     const double2 cS = lds2(sm + c), cW = lds2(sm + HN + c), cE = lds2(sm + 2 * HN + c),
@@ -480,18 +506,18 @@ __device__ __forceinline__ void tile_sweep(const double* sm, const double* xp, d
 }
 
 // Sweeps T..Tp of a pass, each followed by a block barrier; xp ends on the last iterate.
-template <int TB, int T, bool RECIP>
+template <int TB, int T, bool RECIP, bool PART>
 __device__ __forceinline__ void tile_sweeps(const double* sm, double*& xp, double*& xn, int Tp,
                                             int cx_lim, int cy_lim, Acc& acc) {
   if constexpr (T <= TB) {
     if (T <= Tp) {
-      tile_sweep<TB, T, RECIP>(sm, xp, xn, cx_lim, cy_lim, acc);
+      tile_sweep<TB, T, RECIP, PART>(sm, xp, xn, cx_lim, cy_lim, acc);
       __syncthreads();
       double* tmp = xp;
       xp = xn;
       // a first sweep that read x^0 = b from b's own tile hands over the x0 buffer
       xn = (tmp == sm + 5 * JTile<TB>::HN) ? const_cast<double*>(sm) + 6 * JTile<TB>::HN : tmp;
-      tile_sweeps<TB, T + 1, RECIP>(sm, xp, xn, Tp, cx_lim, cy_lim, acc);
+      tile_sweeps<TB, T + 1, RECIP, PART>(sm, xp, xn, Tp, cx_lim, cy_lim, acc);
     }
   }
 }
@@ -525,6 +551,88 @@ __device__ __forceinline__ void acc_reduce(Acc& acc, unsigned long long (*s_acc)
   }
 }
 
+// The tile's haloed box (JBX + 2TB) x (JBY + 2TB) of the system and of the iterate
+// into shared memory (b's tile holds x^0 on a first pass).  PART (a tile cut by the
+// grid's edge): only the (cx_lim + 2TB) x (cy_lim + 2TB) box its sweeps read.
+template <int TB, bool RECIP, bool PART>
+__device__ __forceinline__ void tile_load(const JacobiArgs& a, const double* xin, double* sm,
+                                          int i0, int j0, int cx_lim, int cy_lim, int pitch,
+                                          bool pairs, bool small, bool from_b) {
+  using G = JTile<TB>;
+  constexpr int HX = G::HX, HY = G::HY, HN = G::HN, NW = JNT / 32;
+  double* sS = sm;
+  double* sW = sS + HN;
+  double* sE = sW + HN;
+  double* sN = sE + HN;
+  double* sD = sN + HN;
+  double* sB = sD + HN;
+  double* x0 = sB + HN;
+  const int nx = a.nx, ny = a.ny;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int wx = PART ? min(HX, cx_lim + 2 * TB) : HX, wy = PART ? min(HY, cy_lim + 2 * TB) : HY;
+  if (pairs) {
+    // even pitch, no multiple wrap: a pair (gi, gi + 1) with gi even and gi + 1 < nx
+    // is one 16-byte copy per array.  With even nx that is every pair; with odd nx
+    // (rows padded to an even pitch) the pair that reaches the seam, and the pairs
+    // of a seam tile's wrapped halo (odd gi), take two 8-byte copies instead.
+    for (int ly = warp; ly < wy; ly += NW) {
+      const int gj = wrap_near(j0 - TB + ly, ny);
+      const size_t row = (size_t)gj * pitch;
+      for (int lp = lane; lp < (wx + 1) / 2; lp += 32) {
+        const int lx = 2 * lp;
+        const int gi = wrap_near(i0 - TB + lx, nx);
+        const size_t g = row + gi;
+        const int c = ly * HX + lx;
+        if (!SWM_IN_RANGE(gi, nx, kChkJacPairs) || !SWM_IN_RANGE(gj, ny, kChkJacPairs))
+          continue;
+        if ((gi & 1) == 0 && gi + 1 < nx) {
+          cp_async16(&sS[c], &a.cS[g]);
+          cp_async16(&sW[c], &a.cW[g]);
+          cp_async16(&sE[c], &a.cE[g]);
+          cp_async16(&sN[c], &a.cN[g]);
+          cp_async16(&sD[c], &a.cD[g]);
+          if (!RECIP || from_b) cp_async16(&sB[c], &a.b[g]);  // RECIP: b only for x^0
+          if (!from_b) cp_async16(&x0[c], &xin[g]);
+        } else {
+#pragma unroll
+          for (int e = 0; e < 2; ++e) {
+            const size_t ge = e == 0 ? g : row + (gi + 1 < nx ? gi + 1 : 0);
+            cp_async8(&sS[c + e], &a.cS[ge]);
+            cp_async8(&sW[c + e], &a.cW[ge]);
+            cp_async8(&sE[c + e], &a.cE[ge]);
+            cp_async8(&sN[c + e], &a.cN[ge]);
+            cp_async8(&sD[c + e], &a.cD[ge]);
+            if (!RECIP || from_b) cp_async8(&sB[c + e], &a.b[ge]);
+            if (!from_b) cp_async8(&x0[c + e], &xin[ge]);
+          }
+        }
+      }
+    }
+    cp_async_wait_all();
+  } else {
+    for (int ly = warp; ly < wy; ly += NW) {
+      int gj = j0 - TB + ly;
+      gj = small ? wrap(gj, ny) : wrap_near(gj, ny);
+      const size_t row = (size_t)gj * pitch;
+      for (int lx = lane; lx < wx; lx += 32) {
+        int gi = i0 - TB + lx;
+        gi = small ? wrap(gi, nx) : wrap_near(gi, nx);
+        const size_t g = row + gi;
+        const int c = ly * HX + lx;
+        if (!SWM_IN_RANGE(gi, nx, kChkJacCells) || !SWM_IN_RANGE(gj, ny, kChkJacCells)) continue;
+        cp_async8(&sS[c], &a.cS[g]);
+        cp_async8(&sW[c], &a.cW[g]);
+        cp_async8(&sE[c], &a.cE[g]);
+        cp_async8(&sN[c], &a.cN[g]);
+        cp_async8(&sD[c], &a.cD[g]);
+        if (!RECIP || from_b) cp_async8(&sB[c], &a.b[g]);
+        if (!from_b) cp_async8(&x0[c], &xin[g]);
+      }
+    }
+    cp_async_wait_all();
+  }
+}
+
 // One stencil pass of Tp <= TB sweeps over every tile of this CTA.  A tile is a
 // JBX x JBY block of cells plus a TB-cell halo in shared memory; sweep t updates
 // the region shrunk by t, so after Tp sweeps the tile interior holds x^{k+Tp},
@@ -535,20 +643,15 @@ __device__ void stencil_tiles(const JacobiArgs& a, const double* xin, double* xo
                               unsigned long long (*s_acc)[3]) {
   using G = JTile<TB>;
   constexpr int HX = G::HX, HY = G::HY, HN = G::HN, NW = JNT / 32;
-  double* sS = sm;
-  double* sW = sS + HN;
-  double* sE = sW + HN;
-  double* sN = sE + HN;
-  double* sD = sN + HN;
-  double* sB = sD + HN;
-  double* x0 = sB + HN;
-  double* x1 = x0 + HN;
-  const int nx = a.nx, ny = a.ny;
+  double* sB = sm + 5 * HN;
+  double* x0 = sm + 6 * HN;
+  double* x1 = sm + 7 * HN;
+  const int nx = a.nx, ny = a.ny, pitch = a.pitch > 0 ? a.pitch : nx;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const bool small = (nx < HX) || (ny < HY);
   // 16-byte pairs need an even first column (i0 - TB), an even row pitch and 16-byte
   // aligned arrays (the allocation-free entry takes the caller's pointers as given)
-  const bool pairs = (TB % 2 == 0) && !small && (nx % 2 == 0) && arrays_aligned16(a, xin);
+  const bool pairs = (TB % 2 == 0) && !small && (pitch % 2 == 0) && arrays_aligned16(a, xin);
   // first pass: x^0 = b, already in the b tile (sweep 1 reads it there)
   const bool from_b = xin == a.b;
   const int tx = (nx + JBX - 1) / JBX, ty = (ny + JBY - 1) / JBY;
@@ -565,52 +668,14 @@ __device__ void stencil_tiles(const JacobiArgs& a, const double* xin, double* xo
       acc_reduce<TB>(acc, s_acc);  // keep the per-thread part sums exact
       since_flush = kPerTile;
     }
-    if (pairs) {
-      // even nx, no multiple wrap: 16-byte pairs (gi even) never straddle the seam
-      for (int ly = warp; ly < HY; ly += NW) {
-        const int gj = wrap_near(j0 - TB + ly, ny);
-        const size_t row = (size_t)gj * nx;
-        for (int lp = lane; lp < HX / 2; lp += 32) {
-          const int lx = 2 * lp;
-          const int gi = wrap_near(i0 - TB + lx, nx);
-          const size_t g = row + gi;
-          const int c = ly * HX + lx;
-          if (!SWM_IN_RANGE(gi, nx - 1, kChkJacPairs) || !SWM_IN_RANGE(gj, ny, kChkJacPairs))
-            continue;
-          cp_async16(&sS[c], &a.cS[g]);
-          cp_async16(&sW[c], &a.cW[g]);
-          cp_async16(&sE[c], &a.cE[g]);
-          cp_async16(&sN[c], &a.cN[g]);
-          cp_async16(&sD[c], &a.cD[g]);
-          if (!RECIP || from_b) cp_async16(&sB[c], &a.b[g]);  // RECIP: b only for x^0
-          if (!from_b) cp_async16(&x0[c], &xin[g]);
-        }
-      }
-      cp_async_wait_all();
-    } else {
-      for (int ly = warp; ly < HY; ly += NW) {
-        int gj = j0 - TB + ly;
-        gj = small ? wrap(gj, ny) : wrap_near(gj, ny);
-        const size_t row = (size_t)gj * nx;
-        for (int lx = lane; lx < HX; lx += 32) {
-          int gi = i0 - TB + lx;
-          gi = small ? wrap(gi, nx) : wrap_near(gi, nx);
-          const size_t g = row + gi;
-          const int c = ly * HX + lx;
-          if (!SWM_IN_RANGE(gi, nx, kChkJacCells) || !SWM_IN_RANGE(gj, ny, kChkJacCells)) continue;
-          // the system is read-only during the solve: 8-byte asynchronous copies;
-          // the iterate, which other CTAs wrote, by a load that bypasses L1
-          cp_async8(&sS[c], &a.cS[g]);
-          cp_async8(&sW[c], &a.cW[g]);
-          cp_async8(&sE[c], &a.cE[g]);
-          cp_async8(&sN[c], &a.cN[g]);
-          cp_async8(&sD[c], &a.cD[g]);
-          if (!RECIP || from_b) cp_async8(&sB[c], &a.b[g]);
-          if (!from_b) x0[c] = __ldcg(&xin[g]);
-        }
-      }
-      cp_async_wait_all();
-    }
+    // ensembles: a tile cut by the grid's edge loads and sweeps only the box it needs
+    // (their grids are small, edge tiles common); the single-grid kernel keeps one
+    // code path, which measured 2% faster with the partial variant compiled out
+    const bool part = ONE_TILE && (cx_lim < JBX || cy_lim < JBY);
+    if (part)
+      tile_load<TB, RECIP, true>(a, xin, sm, i0, j0, cx_lim, cy_lim, pitch, pairs, small, from_b);
+    else
+      tile_load<TB, RECIP, false>(a, xin, sm, i0, j0, cx_lim, cy_lim, pitch, pairs, small, from_b);
     __syncthreads();
     if (first) {  // initial residual mean|0 - b| (jacobi_iteration.f90:69)
       for (int ly = TB + warp; ly < TB + JBY; ly += NW)
@@ -619,13 +684,16 @@ __device__ void stencil_tiles(const JacobiArgs& a, const double* xin, double* xo
     }
     double* xp = from_b ? sB : x0;
     double* xn = x1;
-    tile_sweeps<TB, 1, RECIP>(sm, xp, xn, Tp, cx_lim, cy_lim, acc);
+    if (part)
+      tile_sweeps<TB, 1, RECIP, true>(sm, xp, xn, Tp, cx_lim, cy_lim, acc);
+    else
+      tile_sweeps<TB, 1, RECIP, false>(sm, xp, xn, Tp, cx_lim, cy_lim, acc);
     for (int ly = TB + warp; ly < TB + JBY; ly += NW) {
       const int gj = j0 + ly - TB;
       if (gj >= ny) continue;
       for (int lx = TB + lane; lx < TB + JBX; lx += 32) {
         const int gi = i0 + lx - TB;
-        if (gi < nx) xout[(size_t)gj * nx + gi] = xp[ly * HX + lx];
+        if (gi < nx) xout[(size_t)gj * pitch + gi] = xp[ly * HX + lx];
       }
     }
     __syncthreads();
@@ -851,9 +919,11 @@ __device__ __forceinline__ bool jacobi_batch_solve(const JacobiBatchArgs& a, dou
     const JacobiArgs& d = a.descs[p];
     const int res = __ldcg(&a.st[p].result);
     const double* src = res == 1 ? d.xa : d.xb;
-    const int n = d.nx * d.ny;
-    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x)
-      d.out[q] = res == 0 ? 0. : __ldcg(&src[q]);
+    const int n = d.nx * d.ny, pitch = d.pitch > 0 ? d.pitch : d.nx;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+      const int s = pitch == d.nx ? q : (q / d.nx) * pitch + q % d.nx;  // padded rows
+      d.out[q] = res == 0 ? 0. : __ldcg(&src[s]);
+    }
   }
   if (blockIdx.x == 0) {
     for (int p = threadIdx.x; p < nsys; p += blockDim.x) {

@@ -15,9 +15,11 @@ pytestmark = pytest.mark.gpu
 
 def members():
     out = []
-    # uneven sizes, odd row pitches among them (their Jacobi tiles take the 8-byte path)
+    # uneven sizes, odd row pitches among them (rows padded to an even pitch for the
+    # Jacobi tiles); 66 and 129 leave edge tiles two and one columns wide, which the
+    # ensemble loads and sweeps as partial tiles and the single grid as full ones
     for name, n in (("vortex", 40), ("dambreak", 57), ("lake", 73), ("island", 50),
-                    ("lake_dry", 41)):
+                    ("lake_dry", 41), ("vortex", 66), ("island", 129)):
         c = cases.case(name, n=n)
         c["well_balanced"] = 0
         out.append(c)
@@ -122,8 +124,10 @@ def test_persistent_and_per_phase_steps_identical(gpu, precision):
 def test_fp64_members_match_the_oracle(gpu):
     # members of uneven size and family, stepped in one ensemble, against the oracle
     swm = gpu
+    # 65 and 130 leave Jacobi edge tiles one and two columns wide
     ms = [cases.case("vortex", n=48, seed=1), cases.case("dambreak", n=70),
-          cases.case("island", n=64), cases.case("lake", n=90)]
+          cases.case("island", n=64), cases.case("lake", n=90), cases.case("vortex", n=65),
+          cases.case("dambreak", n=130)]
     for c in ms:
         c["well_balanced"] = 0
     b = swm.Batch([params(swm, c, "fp64", 0) for c in ms])

@@ -165,6 +165,30 @@ def test_steps_exact_bitwise_wide(gpu, name):
     assert list(s.stats()["jacobi_iters"][:13]) == list(o.last_jacobi_iters()[:13])
 
 
+@pytest.mark.parametrize("nx,ny", [(65, 17), (66, 33), (129, 18), (130, 47), (67, 31)])
+@pytest.mark.parametrize("block", [2, 4, 8])
+def test_jacobi_bitwise_ragged_tiles(gpu, nx, ny, block):
+    # edge tiles 1, 2, 3 columns wide and 1, 2, 15 rows high (64x16 tiles) hanging
+    # over the grid's edge, even and odd row pitches; a slowly converging system, so
+    # that every pass runs its full block of sweeps
+    c = cases.case("vortex", n=nx)
+    o = O.Oracle(O.make_params(nx, ny, c["x0"], c["x1"], g=c["g"], cfl=c["cfl"]))
+    s = gpu.Solver(nx=nx, ny=ny, x0=c["x0"], x1=c["x1"], g=c["g"], cfl=c["cfl"],
+                   precision="fp64", solver="stencil", jacobi_block=block)
+    rng = np.random.default_rng(nx * 1000 + ny)
+    mass = -0.24 * rng.random((nx * ny, 5))
+    mass[:, 2] = 0.0
+    diag = 1.0 + 0.05 * rng.random(nx * ny)
+    rhs = 0.5 + rng.random(nx * ny)
+    mass = mass.reshape(-1).copy()
+    ref, k_ref = o.jacobi(mass, diag, rhs)
+    got, k, rc = s.debug_jacobi(mass, diag, rhs)
+    assert k_ref > 3 * block
+    assert k == k_ref
+    assert np.array_equal(got, ref)
+    s.close()
+
+
 @pytest.mark.parametrize("maxiter", [1, 2, 3, 5, 6, 7, 9, 1000])
 @pytest.mark.parametrize("block", [2, 4])
 def test_jacobi_planned_passes_vs_maxiter(gpu, maxiter, block):
