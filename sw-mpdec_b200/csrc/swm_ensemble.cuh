@@ -69,34 +69,52 @@ static __device__ __noinline__ void ens_tile(const RhsArgs& a, int i0, int j0) {
   rhs_tile<MODE>(a, nullptr, i0, j0);
 }
 
-// The RHS of descriptor sets set0 .. set0 + nsets - 1 for every (problem, tile); CTAs
-// take tiles one at a time from the counter *ctr (the next one fetched while the
-// current one runs), which balances the phase across SMs.
+// The RHS of descriptor sets set0 .. set0 + nsets - 1 for every (problem, tile).  CTAs
+// take chunks of kRhsChunk consecutive tiles from the counter *ctr (the next chunk
+// fetched while this one runs), which balances the phase across SMs; a chunk's items
+// come in one round trip, and a problem's descriptor is staged again only when the
+// problem changes (consecutive tiles mostly share it), so no tile waits on dependent
+// global loads before it starts.
+constexpr int kRhsChunk = 4;
 template <int MODE>
 __device__ __forceinline__ void ens_rhs(const EnsembleArgs& a, int set0, int nsets,
                                         unsigned int* ctr) {
   __shared__ __align__(16) RhsArgs sr;
+  __shared__ int4 s_items[kRhsChunk];
   __shared__ int s_next;
   static_assert(sizeof(RhsArgs) % 8 == 0 && sizeof(RhsArgs) / 8 <= JNT, "descriptor copy");
   const int total = nsets * a.nrtiles;
-  if (threadIdx.x == 0) s_next = atomicAdd(ctr, 1u);
+  int staged = -1;  // (set0 + set) * nprob + problem of the descriptor in sr
+  if (threadIdx.x == 0) s_next = (int)atomicAdd(ctr, 1u) * kRhsChunk;
   __syncthreads();
-  for (int w = s_next; w < total; w = s_next) {
-    const int set = w / a.nrtiles;
-    const int4 t = a.rtiles[w - set * a.nrtiles];
-    if (!SWM_IN_RANGE(t.x, a.nprob, kChkEnsItem)) {
-      __syncthreads();
-      if (threadIdx.x == 0) s_next = atomicAdd(ctr, 1u);
-      __syncthreads();
-      continue;
+  for (int w0 = s_next; w0 < total; w0 = s_next) {
+    if (threadIdx.x < kRhsChunk) {
+      const int w = w0 + threadIdx.x;
+      int4 t = make_int4(-1, 0, 0, 0);
+      if (w < total) {
+        const int set = w / a.nrtiles;
+        t = a.rtiles[w - set * a.nrtiles];
+        t.w = set;
+      }
+      s_items[threadIdx.x] = t;
     }
-    if (threadIdx.x < sizeof(RhsArgs) / 8)
-      reinterpret_cast<unsigned long long*>(&sr)[threadIdx.x] = reinterpret_cast<
-          const unsigned long long*>(&a.rhs[(size_t)(set0 + set) * a.nprob + t.x])[threadIdx.x];
-    __syncthreads();  // sr staged; every thread has read s_next
-    if (threadIdx.x == 0) s_next = atomicAdd(ctr, 1u);
-    ens_tile<MODE>(sr, t.y, t.z);
-    __syncthreads();  // the tile is done with sr and the dynamic shared memory
+    __syncthreads();  // the chunk's items staged; every thread has read s_next
+    if (threadIdx.x == 0) s_next = (int)atomicAdd(ctr, 1u) * kRhsChunk;
+    for (int q = 0; q < kRhsChunk; ++q) {
+      const int4 t = s_items[q];
+      if (t.x < 0) break;
+      if (!SWM_IN_RANGE(t.x, a.nprob, kChkEnsItem)) continue;
+      const int key = (set0 + t.w) * a.nprob + t.x;
+      if (key != staged) {
+        if (threadIdx.x < sizeof(RhsArgs) / 8)
+          reinterpret_cast<unsigned long long*>(&sr)[threadIdx.x] =
+              reinterpret_cast<const unsigned long long*>(&a.rhs[key])[threadIdx.x];
+        __syncthreads();
+        staged = key;
+      }
+      ens_tile<MODE>(sr, t.y, t.z);
+      __syncthreads();  // the tile is done with sr and the dynamic shared memory
+    }
   }
 }
 
@@ -116,6 +134,7 @@ static __device__ __forceinline__ void ens_assemble(const EnsembleArgs& a, int k
   // descriptors, which stay staged)
   constexpr int kChunk = 8;
   __shared__ __align__(16) unsigned long long sdesc[kWords];
+  __shared__ int2 s_cells[kChunk];
   __shared__ int s_next;
   const bool fused = FAST && nsub == kMaxFusedStages;
   unsigned int* ctr = a.work + 5 + (k - 1);
@@ -123,11 +142,13 @@ static __device__ __forceinline__ void ens_assemble(const EnsembleArgs& a, int k
   if (threadIdx.x == 0) s_next = (int)atomicAdd(ctr, 1u) * kChunk;
   __syncthreads();
   for (int b0 = s_next; b0 < a.ncells; b0 = s_next) {
-    __syncthreads();  // every thread has read s_next
+    if (threadIdx.x < kChunk && b0 + (int)threadIdx.x < a.ncells)
+      s_cells[threadIdx.x] = a.cells[b0 + threadIdx.x];  // the chunk's blocks at once
+    __syncthreads();  // every thread has read s_next; the blocks are staged
     if (threadIdx.x == 0) s_next = (int)atomicAdd(ctr, 1u) * kChunk;
     const int b1 = b0 + kChunk < a.ncells ? b0 + kChunk : a.ncells;
     for (int b = b0; b < b1; ++b) {
-      const int2 w = a.cells[b];
+      const int2 w = s_cells[b - b0];
       if (w.x != staged) {  // stage this problem's descriptors
         __syncthreads();
         if (fused) {

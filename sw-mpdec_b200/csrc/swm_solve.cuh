@@ -787,6 +787,8 @@ static __device__ void batch_decide(const JacobiBatchArgs& a, int blk, int* s_cn
   }
 }
 
+constexpr int kJacChunk = 4;  // work items per counter fetch of a batched solve
+
 // One batched solve of a.nsets x a.nprob independent systems (system set q, problem
 // p -> system q * nprob + p, descriptor descs[system]); every CTA of the grid takes
 // part and every grid barrier is passed by all of them.  Returns false when a
@@ -797,6 +799,7 @@ __device__ __forceinline__ bool jacobi_batch_solve(const JacobiBatchArgs& a, dou
   __shared__ unsigned long long s_acc[kMaxBlock + 1][3];
   __shared__ __align__(16) JacobiArgs sd;
   __shared__ int s_ok, s_cnt, s_p, s_active, s_Tp, s_first, s_cur, s_next;
+  __shared__ int2 s_items[kJacChunk];  // a chunk's (system, tile) items
   static_assert(sizeof(JacobiArgs) % 8 == 0 && sizeof(JacobiArgs) / 8 <= JNT, "descriptor copy");
   const int blk = a.block < 1 ? 1 : (a.block > TB ? TB : a.block);
   const int nsys = a.nsets * a.nprob, nwork = a.nsets * a.ntiles;
@@ -862,22 +865,26 @@ __device__ __forceinline__ bool jacobi_batch_solve(const JacobiBatchArgs& a, dou
   };
   for (;;) {
     if (a.work) {
-      // chunks of kChunk consecutive work items taken one ahead from the shared
-      // counter (dynamic balance); a system stays staged, and its sums in the thread
-      // accumulators, while consecutive items belong to it
-      constexpr int kChunk = 4;
+      // chunks of kJacChunk consecutive work items taken one ahead from the shared
+      // counter (dynamic balance), their items read in one round trip; a system stays
+      // staged, and its sums in the thread accumulators, while consecutive items
+      // belong to it
       __syncthreads();
-      if (threadIdx.x == 0) s_next = (int)atomicAdd(a.work, 1u) * kChunk;
+      if (threadIdx.x == 0) s_next = (int)atomicAdd(a.work, 1u) * kJacChunk;
       __syncthreads();
       int cur = -1, since = 0;
       for (int w0 = s_next; w0 < nwork; w0 = s_next) {
-        __syncthreads();  // every thread has read s_next
-        if (threadIdx.x == 0) s_next = (int)atomicAdd(a.work, 1u) * kChunk;
-        const int w1 = w0 + kChunk < nwork ? w0 + kChunk : nwork;
-        for (int w = w0; w < w1; ++w) {
-          const int set = w / a.ntiles;
+        if (threadIdx.x < kJacChunk && w0 + (int)threadIdx.x < nwork) {
+          const int w = w0 + threadIdx.x, set = w / a.ntiles;
           const int2 t = a.tiles[w - set * a.ntiles];
-          const int sys = set * a.nprob + t.x;
+          s_items[threadIdx.x] = make_int2(set * a.nprob + t.x, t.y);
+        }
+        __syncthreads();  // every thread has read s_next; the items are staged
+        if (threadIdx.x == 0) s_next = (int)atomicAdd(a.work, 1u) * kJacChunk;
+        const int w1 = w0 + kJacChunk < nwork ? w0 + kJacChunk : nwork;
+        for (int w = w0; w < w1; ++w) {
+          const int2 it = s_items[w - w0];  // (system, tile)
+          const int sys = it.x;
           if (sys != cur || since + kPerTile > kAccFlushCells) {
             if (cur >= 0) flush();
             stage(sys);
@@ -885,7 +892,7 @@ __device__ __forceinline__ bool jacobi_batch_solve(const JacobiBatchArgs& a, dou
             since = 0;
           }
           if (s_active) {
-            tile(t.y);
+            tile(it.y);
             since += kPerTile;
           }
         }
