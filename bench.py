@@ -464,8 +464,9 @@ def main():
                "ms_per_step": ms_e2e / args.steps}
         s.close()
 
-    # ensemble: 256 problems of uneven size in one batch (split, autotuned Jacobi
-    # sweeps per pass); under torchrun the problem list is sharded across ranks
+    # ensemble: 256 problems of uneven size in one batch (split; the step form and the
+    # Jacobi sweeps per pass autotuned); under torchrun the problem list is sharded
+    # across ranks
     ens = None
     if not args.no_ensemble:
         members = cases.ensemble(seed=0)
@@ -481,8 +482,15 @@ def main():
         for _ in range(max(args.warmup, 1)):  # the first step also picks the schedule
             bt.step()
         st = torch.cuda.ExternalStream(bt.stream())
+        # every timed run below starts from this state (the Jacobi sweeps depend on it)
+        snap = [bt.get_planes(k) for k in range(len(mine))]
+
+        def restore():
+            for k, P in enumerate(snap):
+                bt.set_planes(k, P)
 
         def time_ensemble():
+            restore()
             barrier()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(st)
@@ -496,23 +504,29 @@ def main():
                                                 dist, device="cuda")
         blk, tot, last = bt.stats()
         launches, ctas = bt.launch_info()
-        phases = bt.phase_times()  # one more step, its phases timed inside the launch
-        # the same ensemble with one launch per phase (40 per step), for comparison
-        bt.set_launches(True)
-        for _ in range(max(args.warmup, 1)):
-            bt.step()
-        ms_phase = replicas.aggregate(time_ensemble(), 0.0, dist, device="cuda")[0]
+        # both step forms fixed in turn, timed from the same state, for comparison
+        forms = {}
+        for name, per_phase in (("persistent", False), ("phased", True)):
+            bt.set_launches(per_phase)
+            bt.step()  # warm the new graph
+            ms_f = replicas.aggregate(time_ensemble(), 0.0, dist, device="cuda")[0]
+            nl, nc = bt.launch_info()
+            forms[name] = {"launches_per_step": nl, "ms_per_step": ms_f / args.steps,
+                           "value": cell_steps / (ms_f * 1e-3)}
+            if not per_phase:
+                forms[name]["ctas"] = nc
+                # one more step from the same state, its phases timed inside the launch
+                restore()
+                forms[name]["phase_ms"] = {k: round(v, 4) for k, v in bt.phase_times().items()}
         ens = {"workload": "256 problems, sides log-uniform in [64,512], vortex / dam break / "
                            "Gaussian lake families, seed 0, split precision",
                "value": cell_steps / (ms_ens * 1e-3), "unit": "cell-steps/s",
                "cells": int(sum(sizes)), "ms_per_step": ms_ens / args.steps,
-               "jacobi_block_autotuned": blk,
+               "schedule": {"form": "persistent" if launches == 1 else "phased",
+                            "jacobi_block": blk, "launches_per_step": launches,
+                            "persistent_ctas": ctas, "chosen_by": "autotuner, first step"},
                "jacobi_iters_per_step_max": int(last.sum(axis=0).max()),
-               "launches_per_step": launches, "persistent_ctas": ctas,
-               "phase_ms": {k: round(v, 4) for k, v in phases.items()},
-               "per_phase_launches": {"launches_per_step": 1 + 13 * 3,
-                                      "ms_per_step": ms_phase / args.steps,
-                                      "value": cell_steps / (ms_phase * 1e-3)}}
+               "forms": forms}
         bt.close()
 
     if rank != 0:

@@ -287,10 +287,14 @@ SWM_API int swm_batch_get_stats(swm_batch_handle b, int *jacobi_block, long long
                                 int *last_iters);
 /* The cudaStream_t the ensemble launches on (for CUDA-event timing by the caller). */
 SWM_API int swm_batch_get_stream(swm_batch_handle b, void **stream);
-/* Debug/measurement: per_phase = 1 steps the ensemble with one launch per phase
- * (40 per step: TimeStep, 13 RHS, 13 assemblies, 13 Jacobi solves, every solve in
- * one system buffer), 0 (default) with the one persistent launch; results are
- * identical.  Resets the captured graph. */
+/* The step form.  per_phase = 1: a kernel per phase, captured in one graph (17 per
+ * step for the split and FMA forms: TimeStep (2), the RHS of U^n, per correction
+ * 1..4 the fused assembly of its three substeps, one batched Jacobi solve of their
+ * systems and one RHS launch over the new substeps, then the last correction's
+ * assembly and solve; 25 for FP64, whose three assemblies are separate); 0: the one
+ * persistent launch; < 0: the autotuner's choice (with jacobi_block = 0 the first
+ * step times both forms; without it the persistent launch).  Results are identical.
+ * Resets the captured graph. */
 SWM_API int swm_batch_debug_set_launches(swm_batch_handle b, int per_phase);
 /* Measurement: one step of every problem (it advances the state) by the persistent
  * launch, recording when its phases end; ms[0..n-1] (cap >= 16) receive the phase
@@ -300,8 +304,8 @@ SWM_API int swm_batch_debug_phase_times(swm_batch_handle b, double *ms, int cap,
 /* Debug: polls of every grid-barrier wait of the ensemble's kernels before the step
  * gives up with SWM_ERR_WATCHDOG (default 2^26; <= 0: at once).  Resets the graph. */
 SWM_API int swm_batch_debug_set_spin_limit(swm_batch_handle b, long long limit);
-/* Launches of the ensemble's own kernels in one step (1 or 40) and the CTAs of the
- * persistent launch (0 when per phase). */
+/* Launches of the ensemble's own kernels in one step (1, or 17 / 25 per phase) and
+ * the CTAs of the persistent launch (0 when per phase). */
 SWM_API int swm_batch_get_launch_info(swm_batch_handle b, int *launches_per_step, int *ctas);
 
 #ifdef __cplusplus

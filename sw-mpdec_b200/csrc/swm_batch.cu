@@ -83,22 +83,22 @@ struct swm_batch {
   cudaStream_t stream = nullptr;
   std::vector<void*> allocs;
   RhsArgs* d_rhs = nullptr;        // [kRhsSets][n]
-  AssembleArgs* d_asm = nullptr;   // [kSolves][n], every solve in system set 0
-  JacobiArgs* d_jac = nullptr;     // [kSolves][n]
-  // persistent step: per-substep systems
+  // per-substep systems (both step forms)
   AssembleArgs* d_asm3 = nullptr;        // [kSolves][n], outputs in the substep's set
   AssembleMultiArgs* d_asmm = nullptr;   // [4][n] fused substeps of corrections 1..4
   JacobiArgs* d_jac5 = nullptr;          // [5][kSubsteps n] systems of each correction
   int2* d_cells256 = nullptr;            // kEnsCells-cell blocks (problem, first cell)
   int ncell256 = 0;
-  bool persistent = true;                // one launch per step (else one per phase)
+  bool persistent = true;                // one launch per step (else a kernel per phase)
+  bool mode_fixed = false;               // the caller chose the step form (no tuning of it)
   long long spin_limit = kDefaultSpinLimit;  // polls of a grid-barrier wait
   int ens_grid = 0;                      // CTAs of the step kernel (autotuned)
   int ens_max[9] = {};                   // co-resident CTAs of the step kernel, per block
   unsigned long long* d_clock = nullptr; // phase timestamps (swm_batch_debug_phase_times)
   unsigned int* d_work = nullptr;        // work-item counters of the step kernel's phases
   bool clocked = false;
-  int4* d_rhs_work = nullptr;
+  int4* d_rhs_work = nullptr;            // RHS tiles (problem, i0, j0, 0)
+  int4* d_rhs_work3 = nullptr;           // the same for three consecutive sets (q n + problem, ...)
   int nrhs = 0;
   int2* d_cells = nullptr;         // 128-cell blocks (problem, first cell)
   int ncellblk = 0;
@@ -284,16 +284,15 @@ static JacobiArgs batch_jac_desc(const swm_batch* b, const BProblem& q, int k, i
 }
 
 // Descriptor tables of the fixed step sequence (the same sequence enqueue_step issues):
-// for the one-launch-per-phase path every solve in system set 0; for the persistent
-// step each substep m of a correction in its own set m - 2 (the last correction's
-// single solve in set 0), the fused substeps of corrections 1..4 (fast forms), and
-// the Jacobi systems of each correction.
+// each substep m of a correction in its own system set m - 2 (the last correction's
+// single solve in set 0), the fused substeps of corrections 1..4 (fast forms), and the
+// Jacobi systems of each correction.
 static int batch_tables(swm_batch* b) {
   const int n = b->n;
   std::vector<RhsArgs> rhs((size_t)kRhsSets * n);
-  std::vector<AssembleArgs> as((size_t)kSolves * n), as3((size_t)kSolves * n);
+  std::vector<AssembleArgs> as3((size_t)kSolves * n);
   std::vector<AssembleMultiArgs> am((size_t)4 * n);
-  std::vector<JacobiArgs> ja((size_t)kSolves * n), ja5((size_t)5 * kSubsteps * n);
+  std::vector<JacobiArgs> ja5((size_t)5 * kSubsteps * n);
   for (int i = 0; i < n; ++i) {
     const BProblem& q = b->pr[i];
     rhs[i] = batch_rhs_desc(q, q.h, q.hu, q.hv, 0);
@@ -306,9 +305,7 @@ static int batch_tables(swm_batch* b) {
       const int mlo = (k == 5) ? 4 : 2;
       for (int m = mlo; m <= 4; ++m, ++solve) {
         const int qs = (k == 5) ? 0 : m - 2;
-        as[(size_t)solve * n + i] = batch_asm_desc(b, q, i, k, m, 0);
         as3[(size_t)solve * n + i] = batch_asm_desc(b, q, i, k, m, qs);
-        ja[(size_t)solve * n + i] = batch_jac_desc(b, q, k, m, 0);
         ja5[((size_t)(k - 1) * kSubsteps + qs) * n + i] = batch_jac_desc(b, q, k, m, qs);
       }
       if (k < 5) {  // the three substeps of this correction fused per cell
@@ -331,8 +328,6 @@ static int batch_tables(swm_batch* b) {
     }
   }
   BCK(cudaMemcpy(b->d_rhs, rhs.data(), sizeof(RhsArgs) * rhs.size(), cudaMemcpyHostToDevice));
-  BCK(cudaMemcpy(b->d_asm, as.data(), sizeof(AssembleArgs) * as.size(), cudaMemcpyHostToDevice));
-  BCK(cudaMemcpy(b->d_jac, ja.data(), sizeof(JacobiArgs) * ja.size(), cudaMemcpyHostToDevice));
   BCK(cudaMemcpy(b->d_asm3, as3.data(), sizeof(AssembleArgs) * as3.size(), cudaMemcpyHostToDevice));
   BCK(cudaMemcpy(b->d_asmm, am.data(), sizeof(AssembleMultiArgs) * am.size(),
                  cudaMemcpyHostToDevice));
@@ -340,41 +335,52 @@ static int batch_tables(swm_batch* b) {
   return SWM_OK;
 }
 
-static cudaError_t batch_rhs(swm_batch* b, int set) {
+// RHS of descriptor set `set` (nsets = 1: the tile list of one set) or of the three
+// consecutive sets set .. set + 2 (nsets = 3) for every problem, in one launch.
+static cudaError_t batch_rhs(swm_batch* b, int set, int nsets) {
   const RhsArgs* d = b->d_rhs + (size_t)set * b->n;
-  if (b->precision == SWM_PREC_FP64) return launch_rhs_batch_exact(d, b->d_rhs_work, b->nrhs, b->stream);
-  return launch_rhs_batch_fast(b->precision == SWM_PREC_SPLIT ? 1 : 0, d, b->d_rhs_work, b->nrhs,
-                               b->stream);
+  const int4* work = nsets == 1 ? b->d_rhs_work : b->d_rhs_work3;
+  const int nw = nsets * b->nrhs;
+  if (b->precision == SWM_PREC_FP64) return launch_rhs_batch_exact(d, work, nw, b->stream);
+  return launch_rhs_batch_fast(b->precision == SWM_PREC_SPLIT ? 1 : 0, d, work, nw, b->stream);
 }
 
-// One mPDeC5 step of every problem (timediscretization.f90:458-566), dt per problem
-// from the batched TimeStep, all on b->stream.
+// One mPDeC5 step of every problem (timediscretization.f90:458-566) as a sequence of
+// kernels, dt per problem from the batched TimeStep, all on b->stream: per correction
+// the assembly of its substeps into their own systems (fast forms: the three fused per
+// cell), one batched Jacobi solve of all of them, and one RHS launch over the three new
+// substeps -- the persistent step's phases and descriptors, phase by phase.
 static int batch_enqueue_phases(swm_batch* b, int block) {
   BCK(cudaMemsetAsync(b->d_ctl, 0, sizeof(JacBatchCtl), b->stream));
   BCK(launch_dt_batch(b->d_dtd, b->d_cells, b->ncellblk, b->n, b->d_lam, b->d_bad, b->d_dt,
                       b->stream));
-  BCK(batch_rhs(b, 0));
+  BCK(batch_rhs(b, 0, 1));
   int solve = 0;
   for (int k = 1; k <= 5; ++k) {
-    const int mlo = (k == 5) ? 4 : 2;
-    for (int m = mlo; m <= 4; ++m, ++solve) {
-      BCK(launch_assemble_batch(b->d_asm + (size_t)solve * b->n, b->d_cells, b->ncellblk, b->fast,
-                                b->stream));
-      JacobiBatchArgs ja{};
-      ja.descs = b->d_jac + (size_t)solve * b->n;
-      ja.tiles = b->d_tiles;
-      ja.ntiles = b->ntiles;
-      ja.nprob = b->n;
-      ja.nsets = 1;
-      ja.st = b->d_st;
-      ja.ctl = b->d_ctl;
-      ja.iters = b->d_iters + (size_t)solve * b->n;
-      ja.block = block;
-      ja.spin_limit = b->spin_limit;
-      BCK(launch_jacobi_batch(ja, b->jac_blocks[block], b->fast, b->stream));
+    const int nsub = (k == 5) ? 1 : kSubsteps;
+    if (b->fast && nsub == kSubsteps) {
+      BCK(launch_assemble_multi_batch(b->d_asmm + (size_t)(k - 1) * b->n, b->d_cells,
+                                      b->ncellblk, b->stream));
+    } else {
+      for (int q = 0; q < nsub; ++q)
+        BCK(launch_assemble_batch(b->d_asm3 + (size_t)(solve + q) * b->n, b->d_cells,
+                                  b->ncellblk, b->fast, b->stream));
     }
-    if (k < 5)
-      for (int m = 2; m <= 4; ++m) BCK(batch_rhs(b, 1 + (k & 1) * 3 + (m - 2)));
+    JacobiBatchArgs ja{};
+    ja.descs = b->d_jac5 + (size_t)(k - 1) * kSubsteps * b->n;
+    ja.tiles = b->d_tiles;
+    ja.ntiles = b->ntiles;
+    ja.nprob = b->n;
+    ja.nsets = nsub;
+    ja.st = b->d_st;
+    ja.ctl = b->d_ctl;
+    ja.iters = b->d_iters + (size_t)solve * b->n;
+    ja.block = block;
+    ja.spin_limit = b->spin_limit;
+    ja.work = b->d_work + 10;  // reset by the solve itself
+    BCK(launch_jacobi_batch(ja, b->jac_blocks[block], b->fast, b->stream));
+    solve += nsub;
+    if (k < 5) BCK(batch_rhs(b, 1 + (k & 1) * kSubsteps, kSubsteps));
   }
   return SWM_OK;
 }
@@ -435,15 +441,15 @@ static int batch_enqueue_persistent(swm_batch* b, int block, int grid) {
   return SWM_OK;
 }
 
-static int batch_enqueue(swm_batch* b, int block, int grid) {
-  return b->persistent ? batch_enqueue_persistent(b, block, grid) : batch_enqueue_phases(b, block);
+static int batch_enqueue(swm_batch* b, bool persistent, int block, int grid) {
+  return persistent ? batch_enqueue_persistent(b, block, grid) : batch_enqueue_phases(b, block);
 }
 
 static int batch_graph(swm_batch* b) {
   if (b->graph) return SWM_OK;
   cudaGraph_t g = nullptr;
   BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-  int rc = batch_enqueue(b, b->block, b->ens_grid);
+  int rc = batch_enqueue(b, b->persistent, b->block, b->ens_grid);
   cudaError_t e = cudaStreamEndCapture(b->stream, &g);
   if (rc) {
     if (g) cudaGraphDestroy(g);
@@ -472,9 +478,11 @@ static int batch_copy_state(swm_batch* b, bool to_save) {
 }
 
 // Autotuner: time one step per candidate schedule on the initial state, restore the
-// state after each, keep the fastest.  Candidates: Jacobi temporal block 2, 4, 8 (the
-// haloed tile of a pass is 64+2T x 16+2T cells) and, for the persistent step, the
-// co-resident grid or half of it (one CTA per SM instead of two).
+// state after each, keep the fastest.  Candidates: the step form (the persistent launch,
+// or a kernel per phase, unless the caller fixed it), the Jacobi temporal block 2, 4, 8
+// (the haloed tile of a pass is 64+2T x 16+2T cells) and, for the persistent step, the
+// co-resident grid or half of it (one CTA per SM instead of two).  Every schedule gives
+// the same results.
 static int batch_tune(swm_batch* b) {
   NvtxRange range("ensemble autotune");
   for (auto& q : b->pr)
@@ -487,24 +495,32 @@ static int batch_tune(swm_batch* b) {
   if (rc) return rc;
   int sms = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
-  std::vector<std::pair<int, int>> cands;  // (block, grid)
-  for (int c : kCandidates) {
-    if (!b->persistent) {
-      cands.emplace_back(c, 0);
-      continue;
+  struct Cand {
+    bool persistent;
+    int block, grid;
+  };
+  std::vector<Cand> cands;
+  for (int form = 0; form < 2; ++form) {
+    const bool pers = form == 0;
+    if (b->mode_fixed && pers != b->persistent) continue;
+    for (int c : kCandidates) {
+      if (!pers) {
+        cands.push_back({false, c, 0});
+        continue;
+      }
+      cands.push_back({true, c, b->ens_max[c]});
+      if (b->ens_max[c] >= 2 * sms) cands.push_back({true, c, b->ens_max[c] / 2});
     }
-    cands.emplace_back(c, b->ens_max[c]);
-    if (b->ens_max[c] >= 2 * sms) cands.emplace_back(c, b->ens_max[c] / 2);
   }
   cudaEvent_t e0, e1;
   BCK(cudaEventCreate(&e0));
   BCK(cudaEventCreate(&e1));
   float best = 1e30f;
-  std::pair<int, int> pick = cands[0];
+  Cand pick = cands[0];
   for (const auto& c : cands) {
     for (int rep = 0; rep < 2; ++rep) {  // first repetition warms the kernels
       BCK(cudaEventRecord(e0, b->stream));
-      if ((rc = batch_enqueue(b, c.first, c.second))) return rc;
+      if ((rc = batch_enqueue(b, c.persistent, c.block, c.grid))) return rc;
       BCK(cudaEventRecord(e1, b->stream));
       BCK(cudaStreamSynchronize(b->stream));
       if ((rc = batch_copy_state(b, false))) return rc;
@@ -519,8 +535,9 @@ static int batch_tune(swm_batch* b) {
   BCK(cudaStreamSynchronize(b->stream));
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  b->block = pick.first;
-  b->ens_grid = pick.second;
+  b->persistent = pick.persistent;
+  b->block = pick.block;
+  b->ens_grid = pick.grid;
   b->autotune = false;
   return SWM_OK;
 }
@@ -592,8 +609,11 @@ int swm_batch_create(int n, const swm_params* p, swm_batch_handle* out) {
   b->ncellblk = (int)cb.size();
   b->ncell256 = (int)cb256.size();
   b->ntiles = (int)tl.size();
-  if ((rc = b->alloc(&b->d_rhs, (size_t)kRhsSets * n)) || (rc = b->alloc(&b->d_asm, (size_t)kSolves * n)) ||
-      (rc = b->alloc(&b->d_jac, (size_t)kSolves * n)) || (rc = b->alloc(&b->d_rhs_work, rw.size())) ||
+  std::vector<int4> rw3;  // the tile list of three consecutive descriptor sets
+  for (int q3 = 0; q3 < kSubsteps; ++q3)
+    for (const int4& t : rw) rw3.push_back(make_int4(q3 * n + t.x, t.y, t.z, 0));
+  if ((rc = b->alloc(&b->d_rhs, (size_t)kRhsSets * n)) || (rc = b->alloc(&b->d_rhs_work, rw.size())) ||
+      (rc = b->alloc(&b->d_rhs_work3, rw3.size())) ||
       (rc = b->alloc(&b->d_cells, cb.size())) || (rc = b->alloc(&b->d_tiles, tl.size())) ||
       (rc = b->alloc(&b->d_dtd, (size_t)n)) || (rc = b->alloc(&b->d_dt, (size_t)n)) ||
       (rc = b->alloc(&b->d_lam, 2 * (size_t)n)) || (rc = b->alloc(&b->d_bad, (size_t)n)) ||
@@ -606,6 +626,7 @@ int swm_batch_create(int n, const swm_params* p, swm_batch_handle* out) {
       (rc = b->alloc(&b->d_iters, (size_t)kSolves * n)))
     return cleanup(rc);
   if (cudaMemcpy(b->d_rhs_work, rw.data(), sizeof(int4) * rw.size(), cudaMemcpyHostToDevice) ||
+      cudaMemcpy(b->d_rhs_work3, rw3.data(), sizeof(int4) * rw3.size(), cudaMemcpyHostToDevice) ||
       cudaMemcpy(b->d_cells, cb.data(), sizeof(int2) * cb.size(), cudaMemcpyHostToDevice) ||
       cudaMemcpy(b->d_tiles, tl.data(), sizeof(int2) * tl.size(), cudaMemcpyHostToDevice) ||
       cudaMemcpy(b->d_cells256, cb256.data(), sizeof(int2) * cb256.size(),
@@ -718,6 +739,11 @@ int swm_batch_debug_set_launches(swm_batch_handle b, int per_phase) {
   BCK(cudaStreamSynchronize(b->stream));
   if (b->graph) cudaGraphExecDestroy(b->graph);
   b->graph = nullptr;
+  if (per_phase < 0) {  // the autotuner's choice (on the first step, if it has not run)
+    b->mode_fixed = false;
+    return SWM_OK;
+  }
+  b->mode_fixed = true;
   b->persistent = per_phase == 0;
   if (!b->persistent && b->block > kMaxBlock) b->block = kMaxBlock;
   return SWM_OK;
@@ -759,7 +785,11 @@ int swm_batch_get_launch_info(swm_batch_handle b, int* launches_per_step, int* c
   if (!b) return bfail(SWM_ERR_PARAM, "null handle");
   const int tb = b->block <= 2 ? 2 : (b->block <= 4 ? 4 : 8);
   const int gmax = b->ens_max[tb];
-  if (launches_per_step) *launches_per_step = b->persistent ? 1 : 1 + 3 * kSolves;
+  // per phase: TimeStep (2), RHS of U^n, per correction 1..4 the assembly (fast forms
+  // fused, else one per substep), the batched solve and the substeps' RHS, then the last
+  // correction's assembly and solve
+  if (launches_per_step)
+    *launches_per_step = b->persistent ? 1 : 2 + 1 + 4 * ((b->fast ? 1 : kSubsteps) + 2) + 2;
   if (ctas)
     *ctas = !b->persistent ? 0 : (b->ens_grid < 1 || b->ens_grid > gmax ? gmax : b->ens_grid);
   return SWM_OK;

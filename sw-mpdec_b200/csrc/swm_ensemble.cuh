@@ -168,23 +168,7 @@ static __device__ __forceinline__ void ens_assemble(const EnsembleArgs& a, int k
       const int c = w.y + threadIdx.x;
       if (fused) {
         const AssembleMultiArgs& am = *reinterpret_cast<const AssembleMultiArgs*>(sdesc);
-        if (c < am.base.nx * am.base.ny) {
-          const int i = c % am.base.nx, j = c / am.base.nx;
-          const size_t kk = (size_t)j * am.base.nx + i, kx = (size_t)j * (am.base.nx + 1) + i;
-          CellIn<4> cin;
-          load_cell<true, 4>(am.base, i, j, kk, kx, cin);
-          double hK[kMaxFusedStages], hL[kMaxFusedStages][4];
-#pragma unroll
-          for (int q = 0; q < kMaxFusedStages; ++q) load_hp(am.base, am.m[q], i, j, hK[q], hL[q]);
-#pragma unroll
-          for (int q = 0; q < kMaxFusedStages; ++q) {
-            const StageOut o{am.hu_out[q], am.hv_out[q], am.cS[q], am.cW[q], am.cE[q], am.cN[q],
-                             am.cD[q]};
-            assemble_stage<true, 4>(am.base, false, i, j, cin, hK[q], hL[q], am.theta[q], o);
-          }
-          // the rhs in the planes' padded layout (odd nx), once per step
-          if (am.base.rhs_out) am.base.rhs_out[(size_t)j * am.base.jpitch + i] = cin.b;
-        }
+        if (c < am.base.nx * am.base.ny) assemble_multi_cell(am, c % am.base.nx, c / am.base.nx);
       } else {
         const AssembleArgs* ad = reinterpret_cast<const AssembleArgs*>(sdesc);
         if (c < ad[0].nx * ad[0].ny)

@@ -167,17 +167,7 @@ __global__ void __launch_bounds__(128, 4) assemble_multi_kernel(const AssembleMu
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y;
   if (i >= a.base.nx || j >= a.base.ny) return;
-  const size_t k = (size_t)j * a.base.nx + i, kx = (size_t)j * (a.base.nx + 1) + i;
-  CellIn<4> c;
-  load_cell<true, 4>(a.base, i, j, k, kx, c);
-  double hK[kMaxFusedStages], hL[kMaxFusedStages][4];
-#pragma unroll
-  for (int q = 0; q < kMaxFusedStages; ++q) load_hp(a.base, a.m[q], i, j, hK[q], hL[q]);
-#pragma unroll
-  for (int q = 0; q < kMaxFusedStages; ++q) {
-    const StageOut o{a.hu_out[q], a.hv_out[q], a.cS[q], a.cW[q], a.cE[q], a.cN[q], a.cD[q]};
-    assemble_stage<true, 4>(a.base, false, i, j, c, hK[q], hL[q], a.theta[q], o);
-  }
+  assemble_multi_cell(a, i, j);
 }
 
 cudaError_t launch_assemble_multi(const AssembleMultiArgs& a, cudaStream_t s) {
@@ -213,6 +203,29 @@ __global__ void __launch_bounds__(128)
     assemble_cell<FAST, 4>(sa, false, c % sa.nx, c / sa.nx);
   else
     assemble_cell<FAST, 2>(sa, false, c % sa.nx, c / sa.nx);
+}
+
+// Ensembles, fast forms: the fused assembly of a correction's three substeps; block b
+// covers 128 cells of problem blk[b].x from blk[b].y (descriptor staged in shared memory).
+__global__ void __launch_bounds__(128, 4)
+    assemble_multi_batch_kernel(const AssembleMultiArgs* __restrict__ descs,
+                                const int2* __restrict__ blk) {
+  static_assert(sizeof(AssembleMultiArgs) % 8 == 0, "copy");
+  __shared__ __align__(16) AssembleMultiArgs sa;
+  const int2 w = blk[blockIdx.x];
+  for (int q = threadIdx.x; q < (int)(sizeof(AssembleMultiArgs) / 8); q += blockDim.x)
+    reinterpret_cast<unsigned long long*>(&sa)[q] =
+        reinterpret_cast<const unsigned long long*>(&descs[w.x])[q];
+  __syncthreads();
+  const int c = w.y + threadIdx.x;
+  if (c < sa.base.nx * sa.base.ny) assemble_multi_cell(sa, c % sa.base.nx, c / sa.base.nx);
+}
+
+cudaError_t launch_assemble_multi_batch(const AssembleMultiArgs* descs, const int2* blk, int nblk,
+                                        cudaStream_t s) {
+  if (nblk < 1) return cudaSuccess;
+  assemble_multi_batch_kernel<<<nblk, 128, 0, s>>>(descs, blk);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_assemble_batch(const AssembleArgs* descs, const int2* blk, int nblk, bool fast,

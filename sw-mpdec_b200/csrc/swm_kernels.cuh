@@ -225,6 +225,8 @@ cudaError_t launch_rhs_batch_fast(int mode, const RhsArgs* descs, const int4* wo
                                   cudaStream_t s);
 cudaError_t launch_rhs_batch_exact(const RhsArgs* descs, const int4* work, int nwork,
                                    cudaStream_t s);
+cudaError_t launch_assemble_multi_batch(const AssembleMultiArgs* descs, const int2* blk, int nblk,
+                                        cudaStream_t s);
 cudaError_t launch_assemble_batch(const AssembleArgs* descs, const int2* blk, int nblk, bool fast,
                                   cudaStream_t s);
 cudaError_t launch_jacobi_batch(const JacobiBatchArgs& a, int grid_blocks, bool recip,

@@ -315,6 +315,28 @@ __device__ __forceinline__ void assemble_cell(const AssembleArgs& a, bool csr, c
   }
 }
 
+// One cell of the fast forms' fused assembly of the kMaxFusedStages substeps of a
+// correction (assemble_kernel's arithmetic per substep, shared inputs loaded once),
+// plus the rhs in the planes' padded layout when rhs_out is set (odd nx, once per step).
+__device__ __forceinline__ void assemble_multi_cell(const AssembleMultiArgs& am, const int i,
+                                                    const int j) {
+  const size_t kk = (size_t)j * am.base.nx + i, kx = (size_t)j * (am.base.nx + 1) + i;
+  CellIn<4> cin;
+  load_cell<true, 4>(am.base, i, j, kk, kx, cin);
+  double hK[kMaxFusedStages], hL[kMaxFusedStages][4];
+#pragma unroll
+  for (int q = 0; q < kMaxFusedStages; ++q) load_hp(am.base, am.m[q], i, j, hK[q], hL[q]);
+#pragma unroll
+  for (int q = 0; q < kMaxFusedStages; ++q) {
+    const StageOut o{am.hu_out[q], am.hv_out[q], am.cS[q], am.cW[q], am.cE[q], am.cN[q], am.cD[q]};
+    assemble_stage<true, 4>(am.base, false, i, j, cin, hK[q], hL[q], am.theta[q], o);
+  }
+  if (am.base.rhs_out) {
+    const size_t kj = am.base.jpitch > 0 ? (size_t)j * am.base.jpitch + i : kk;
+    am.base.rhs_out[kj] = cin.b;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Jacobi (jacobi_iteration.f90:52-87): x^{k+1} = (b - L x^k)/D from x^0 = b,
 // residual mean|x^{k+1}-x^k|, stop when <= tol or at maxIter.

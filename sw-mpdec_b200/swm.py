@@ -397,8 +397,11 @@ class Batch:
         return p.value or 0
 
     def set_launches(self, per_phase):
-        """One launch per phase (True, 40 per step) or the persistent step (False)."""
-        _check(self.lib.swm_batch_debug_set_launches(self.h, 1 if per_phase else 0))
+        """The step form: a kernel per phase (True; 17 launches per step for the split
+        and FMA forms, 25 for FP64), the persistent launch (False), or the autotuner's
+        choice (None)."""
+        v = -1 if per_phase is None else (1 if per_phase else 0)
+        _check(self.lib.swm_batch_debug_set_launches(self.h, v))
 
     def phase_times(self):
         """Durations (ms) of the persistent step's phases over one step (which advances

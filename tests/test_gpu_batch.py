@@ -98,7 +98,7 @@ def test_batch_is_one_launch_per_step(gpu):
     launches, ctas = b.launch_info()
     assert launches == 1 and ctas >= 148
     b.set_launches(True)
-    assert b.launch_info() == (40, 0)
+    assert b.launch_info() == (17, 0)
     b.close()
 
 
@@ -119,6 +119,38 @@ def test_persistent_and_per_phase_steps_identical(gpu, precision):
         assert np.array_equal(a, c)
     assert all(np.array_equal(x, y) for x, y in zip(outs[0][1], outs[1][1]))
     assert np.array_equal(outs[0][2], outs[1][2])
+
+
+def test_autotuned_step_form_matches_fixed_forms(gpu):
+    # jacobi_block = 0: the first step times the persistent and the per-phase forms (and
+    # the sweeps per pass), restoring the state after each; whichever it keeps, the
+    # steps equal those of a batch with the form and block fixed
+    swm = gpu
+    ms = members()[:4]
+    outs = []
+    for block, per_phase in ((0, None), (4, False)):
+        b = swm.Batch([params(swm, c, "split", block) for c in ms])
+        b.set_launches(per_phase)
+        for i, c in enumerate(ms):
+            b.set_planes(i, cases.cell_averages(c))
+        for _ in range(2):
+            b.step()
+        if block == 0:
+            assert b.launch_info()[0] in (1, 17)
+        outs.append([b.get_planes(i) for i in range(len(ms))])
+        b.close()
+    for x, y in zip(*outs):
+        assert np.array_equal(x, y)
+
+
+def test_per_phase_launch_counts(gpu):
+    swm = gpu
+    ms = members()[:2]
+    for precision, n in (("split", 17), ("fp64_fma", 17), ("fp64", 25)):
+        b = swm.Batch([params(swm, c, precision, 4) for c in ms])
+        b.set_launches(True)
+        assert b.launch_info() == (n, 0), precision
+        b.close()
 
 
 def test_fp64_members_match_the_oracle(gpu):
