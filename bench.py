@@ -351,6 +351,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--ensemble-only", action="store_true")  # profiling runs
     ap.add_argument("--no-accuracy", action="store_true")  # profiling runs: no wet-dry leg
     ap.add_argument("--n", type=int, default=2048)
     # profiling runs only: a subset of the timed forms, or another time scheme (its
@@ -388,6 +389,79 @@ def main():
 
     def max_over_ranks(x):
         return replicas.aggregate(x, 0.0, dist, device="cuda")[0]
+
+    def ensemble_leg():
+        # ensemble: 256 problems of uneven size in one batch (split; the step form and the
+        # Jacobi sweeps per pass autotuned); under torchrun the problem list is sharded
+        # across ranks
+        members = cases.ensemble(seed=0)
+        sizes = [m["nx"] * m["ny"] for m in members]
+        mine = replicas.shard(sizes, rank, world)
+        plist = [swm.make_params(m["nx"], m["ny"], m["x0"], m["x1"], g=m["g"], cfl=m["cfl"],
+                                 bathy_flag=m["bathy_flag"], bathy_par=m["bathy_par"],
+                                 precision="split", solver="stencil", jacobi_block=0,
+                                 device=local) for m in (members[i] for i in mine)]
+        bt = swm.Batch(plist)
+        for k, i in enumerate(mine):
+            bt.set_planes(k, cases.cell_averages(members[i]))
+        for _ in range(max(args.warmup, 1)):  # the first step also picks the schedule
+            bt.step()
+        st = torch.cuda.ExternalStream(bt.stream())
+        # every timed run below starts from this state (the Jacobi sweeps depend on it)
+        snap = [bt.get_planes(k) for k in range(len(mine))]
+
+        def restore():
+            for k, P in enumerate(snap):
+                bt.set_planes(k, P)
+
+        def time_ensemble():
+            restore()
+            barrier()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            for _ in range(args.steps):
+                bt.step()
+            e1.record(st)
+            torch.cuda.synchronize()
+            return e0.elapsed_time(e1)
+
+        ms_ens, cell_steps = replicas.aggregate(time_ensemble(), bt.cells() * args.steps,
+                                                dist, device="cuda")
+        blk, tot, last = bt.stats()
+        launches, ctas = bt.launch_info()
+        # both step forms fixed in turn, timed from the same state, for comparison
+        forms = {}
+        for name, per_phase in (("persistent", False), ("phased", True)):
+            bt.set_launches(per_phase)
+            bt.step()  # warm the new graph
+            ms_f = replicas.aggregate(time_ensemble(), 0.0, dist, device="cuda")[0]
+            nl, nc = bt.launch_info()
+            forms[name] = {"launches_per_step": nl, "ms_per_step": ms_f / args.steps,
+                           "value": cell_steps / (ms_f * 1e-3)}
+            if not per_phase:
+                forms[name]["ctas"] = nc
+                # one more step from the same state, its phases timed inside the launch
+                restore()
+                forms[name]["phase_ms"] = {k: round(v, 4) for k, v in bt.phase_times().items()}
+        ens = {"workload": "256 problems, sides log-uniform in [64,512], vortex / dam break / "
+                           "Gaussian lake families, seed 0, split precision",
+               "value": cell_steps / (ms_ens * 1e-3), "unit": "cell-steps/s",
+               "cells": int(sum(sizes)), "ms_per_step": ms_ens / args.steps,
+               "schedule": {"form": "persistent" if launches == 1 else "phased",
+                            "jacobi_block": blk, "launches_per_step": launches,
+                            "persistent_ctas": ctas, "chosen_by": "autotuner, first step"},
+               "jacobi_iters_per_step_max": int(last.sum(axis=0).max()),
+               "forms": forms}
+        bt.close()
+        return ens
+
+    if args.ensemble_only:  # profiling runs: the ensemble leg alone
+        ens = ensemble_leg()
+        if rank == 0:
+            print(json.dumps({"profiling_run": True, "ensemble": ens}), flush=True)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
 
     results = {}
     clocks = None
@@ -464,70 +538,7 @@ def main():
                "ms_per_step": ms_e2e / args.steps}
         s.close()
 
-    # ensemble: 256 problems of uneven size in one batch (split; the step form and the
-    # Jacobi sweeps per pass autotuned); under torchrun the problem list is sharded
-    # across ranks
-    ens = None
-    if not args.no_ensemble:
-        members = cases.ensemble(seed=0)
-        sizes = [m["nx"] * m["ny"] for m in members]
-        mine = replicas.shard(sizes, rank, world)
-        plist = [swm.make_params(m["nx"], m["ny"], m["x0"], m["x1"], g=m["g"], cfl=m["cfl"],
-                                 bathy_flag=m["bathy_flag"], bathy_par=m["bathy_par"],
-                                 precision="split", solver="stencil", jacobi_block=0,
-                                 device=local) for m in (members[i] for i in mine)]
-        bt = swm.Batch(plist)
-        for k, i in enumerate(mine):
-            bt.set_planes(k, cases.cell_averages(members[i]))
-        for _ in range(max(args.warmup, 1)):  # the first step also picks the schedule
-            bt.step()
-        st = torch.cuda.ExternalStream(bt.stream())
-        # every timed run below starts from this state (the Jacobi sweeps depend on it)
-        snap = [bt.get_planes(k) for k in range(len(mine))]
-
-        def restore():
-            for k, P in enumerate(snap):
-                bt.set_planes(k, P)
-
-        def time_ensemble():
-            restore()
-            barrier()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(st)
-            for _ in range(args.steps):
-                bt.step()
-            e1.record(st)
-            torch.cuda.synchronize()
-            return e0.elapsed_time(e1)
-
-        ms_ens, cell_steps = replicas.aggregate(time_ensemble(), bt.cells() * args.steps,
-                                                dist, device="cuda")
-        blk, tot, last = bt.stats()
-        launches, ctas = bt.launch_info()
-        # both step forms fixed in turn, timed from the same state, for comparison
-        forms = {}
-        for name, per_phase in (("persistent", False), ("phased", True)):
-            bt.set_launches(per_phase)
-            bt.step()  # warm the new graph
-            ms_f = replicas.aggregate(time_ensemble(), 0.0, dist, device="cuda")[0]
-            nl, nc = bt.launch_info()
-            forms[name] = {"launches_per_step": nl, "ms_per_step": ms_f / args.steps,
-                           "value": cell_steps / (ms_f * 1e-3)}
-            if not per_phase:
-                forms[name]["ctas"] = nc
-                # one more step from the same state, its phases timed inside the launch
-                restore()
-                forms[name]["phase_ms"] = {k: round(v, 4) for k, v in bt.phase_times().items()}
-        ens = {"workload": "256 problems, sides log-uniform in [64,512], vortex / dam break / "
-                           "Gaussian lake families, seed 0, split precision",
-               "value": cell_steps / (ms_ens * 1e-3), "unit": "cell-steps/s",
-               "cells": int(sum(sizes)), "ms_per_step": ms_ens / args.steps,
-               "schedule": {"form": "persistent" if launches == 1 else "phased",
-                            "jacobi_block": blk, "launches_per_step": launches,
-                            "persistent_ctas": ctas, "chosen_by": "autotuner, first step"},
-               "jacobi_iters_per_step_max": int(last.sum(axis=0).max()),
-               "forms": forms}
-        bt.close()
+    ens = None if args.no_ensemble else ensemble_leg()
 
     if rank != 0:
         if dist is not None:
