@@ -296,10 +296,12 @@ SWM_API int swm_batch_get_stream(swm_batch_handle b, void **stream);
  * step times both forms; without it the persistent launch).  Results are identical.
  * Resets the captured graph. */
 SWM_API int swm_batch_debug_set_launches(swm_batch_handle b, int per_phase);
-/* Measurement: one step of every problem (it advances the state) by the persistent
- * launch, recording when its phases end; ms[0..n-1] (cap >= 16) receive the phase
- * durations: TimeStep, RHS of U^n, then per correction k = 1..5 the assembly, the
- * Jacobi solve and (k < 5) the RHS of the new substeps. */
+/* Measurement: one step of every problem (it advances the state) in the current form,
+ * recording when its phases end (the persistent launch by a global timer read at each
+ * phase's closing barrier, the per-phase form by CUDA events between its kernels);
+ * ms[0..n-1] (cap >= 16) receive the phase durations: TimeStep, RHS of U^n, then per
+ * correction k = 1..5 the assembly, the Jacobi solve and (k < 5) the RHS of the new
+ * substeps. */
 SWM_API int swm_batch_debug_phase_times(swm_batch_handle b, double *ms, int cap, int *n);
 /* Debug: polls of every grid-barrier wait of the ensemble's kernels before the step
  * gives up with SWM_ERR_WATCHDOG (default 2^26; <= 0: at once).  Resets the graph. */

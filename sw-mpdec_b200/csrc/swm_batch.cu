@@ -350,11 +350,20 @@ static cudaError_t batch_rhs(swm_batch* b, int set, int nsets) {
 // the assembly of its substeps into their own systems (fast forms: the three fused per
 // cell), one batched Jacobi solve of all of them, and one RHS launch over the three new
 // substeps -- the persistent step's phases and descriptors, phase by phase.
-static int batch_enqueue_phases(swm_batch* b, int block) {
+// marks (measurement, uncaptured): an event recorded before the step and after each
+// phase, the persistent step's phase boundaries (kEnsMarks events).
+static int batch_enqueue_phases(swm_batch* b, int block, cudaEvent_t* marks = nullptr) {
+  int mk = 0;
+  auto mark = [&]() -> cudaError_t {
+    return marks ? cudaEventRecord(marks[mk++], b->stream) : cudaSuccess;
+  };
+  BCK(mark());
   BCK(cudaMemsetAsync(b->d_ctl, 0, sizeof(JacBatchCtl), b->stream));
   BCK(launch_dt_batch(b->d_dtd, b->d_cells, b->ncellblk, b->n, b->d_lam, b->d_bad, b->d_dt,
                       b->stream));
+  BCK(mark());
   BCK(batch_rhs(b, 0, 1));
+  BCK(mark());
   int solve = 0;
   for (int k = 1; k <= 5; ++k) {
     const int nsub = (k == 5) ? 1 : kSubsteps;
@@ -366,6 +375,7 @@ static int batch_enqueue_phases(swm_batch* b, int block) {
         BCK(launch_assemble_batch(b->d_asm3 + (size_t)(solve + q) * b->n, b->d_cells,
                                   b->ncellblk, b->fast, b->stream));
     }
+    BCK(mark());
     JacobiBatchArgs ja{};
     ja.descs = b->d_jac5 + (size_t)(k - 1) * kSubsteps * b->n;
     ja.tiles = b->d_tiles;
@@ -379,8 +389,12 @@ static int batch_enqueue_phases(swm_batch* b, int block) {
     ja.spin_limit = b->spin_limit;
     ja.work = b->d_work + 10;  // reset by the solve itself
     BCK(launch_jacobi_batch(ja, b->jac_blocks[block], b->fast, b->stream));
+    BCK(mark());
     solve += nsub;
-    if (k < 5) BCK(batch_rhs(b, 1 + (k & 1) * kSubsteps, kSubsteps));
+    if (k < 5) {
+      BCK(batch_rhs(b, 1 + (k & 1) * kSubsteps, kSubsteps));
+      BCK(mark());
+    }
   }
   return SWM_OK;
 }
@@ -752,11 +766,26 @@ int swm_batch_debug_set_launches(swm_batch_handle b, int per_phase) {
 int swm_batch_debug_phase_times(swm_batch_handle b, double* ms, int cap, int* n) {
   NvtxRange range("swm_batch_debug_phase_times");
   if (!b || !ms || cap < kEnsMarks - 1) return bfail(SWM_ERR_PARAM, "invalid argument");
-  if (!b->persistent) return bfail(SWM_ERR_STATE, "phase times need the persistent step");
   if (!b->have_state) return bfail(SWM_ERR_STATE, "no state set");
   BCK(cudaSetDevice(b->device));
   int rc;
   if (b->autotune && (rc = batch_tune(b))) return rc;
+  if (!b->persistent) {  // per-phase form: CUDA events between its kernels
+    cudaEvent_t ev[kEnsMarks] = {};
+    for (auto& e : ev) BCK(cudaEventCreate(&e));
+    rc = batch_enqueue_phases(b, b->block, ev);
+    if (!rc) {
+      BCK(cudaStreamSynchronize(b->stream));
+      for (int i = 0; i + 1 < kEnsMarks; ++i) {
+        float f = 0.f;
+        BCK(cudaEventElapsedTime(&f, ev[i], ev[i + 1]));
+        ms[i] = f;
+      }
+      if (n) *n = kEnsMarks - 1;
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    return rc;
+  }
   if (!b->d_clock && (rc = b->alloc(&b->d_clock, kEnsMarks))) return rc;
   BCK(cudaMemsetAsync(b->d_clock, 0, sizeof(unsigned long long) * kEnsMarks, b->stream));
   b->clocked = true;

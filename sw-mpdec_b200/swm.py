@@ -404,8 +404,9 @@ class Batch:
         _check(self.lib.swm_batch_debug_set_launches(self.h, v))
 
     def phase_times(self):
-        """Durations (ms) of the persistent step's phases over one step (which advances
-        the state): TimeStep, RHS of U^n, then per correction assembly, Jacobi, RHS."""
+        """Durations (ms) of the step's phases over one step in the current form (which
+        advances the state): TimeStep, RHS of U^n, then per correction assembly,
+        Jacobi, RHS."""
         ms = np.zeros(32)
         n = ctypes.c_int()
         _check(self.lib.swm_batch_debug_phase_times(self.h, _dp(ms), 32, ctypes.byref(n)))

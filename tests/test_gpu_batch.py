@@ -143,6 +143,29 @@ def test_autotuned_step_form_matches_fixed_forms(gpu):
         assert np.array_equal(x, y)
 
 
+def test_phase_times_step_like_a_step_in_both_forms(gpu):
+    # the timed step of either form advances the state exactly as step() does
+    swm = gpu
+    ms = members()[:3]
+    outs = []
+    for how in ("step", "persistent", "phased"):
+        b = swm.Batch([params(swm, c, "split", 4) for c in ms])
+        if how != "step":
+            b.set_launches(how == "phased")
+        for i, c in enumerate(ms):
+            b.set_planes(i, cases.cell_averages(c))
+        if how == "step":
+            b.step()
+        else:
+            pt = b.phase_times()
+            assert len(pt) == 16 and all(v > 0.0 for v in pt.values()), (how, pt)
+        outs.append([b.get_planes(i) for i in range(len(ms))])
+        b.close()
+    for other in outs[1:]:
+        for x, y in zip(outs[0], other):
+            assert np.array_equal(x, y)
+
+
 def test_per_phase_launch_counts(gpu):
     swm = gpu
     ms = members()[:2]
