@@ -99,7 +99,10 @@ __device__ __forceinline__ void ens_rhs(const EnsembleArgs& a, int set0, int nse
       s_items[threadIdx.x] = t;
     }
     __syncthreads();  // the chunk's items staged; every thread has read s_next
-    if (threadIdx.x == 0) s_next = (int)atomicAdd(ctr, 1u) * kRhsChunk;
+    // the next chunk, fetched now and published at the chunk's end, so that no thread
+    // waits for the atomic before the chunk's work
+    int nxt = 0;
+    if (threadIdx.x == 0) nxt = (int)atomicAdd(ctr, 1u) * kRhsChunk;
     for (int q = 0; q < kRhsChunk; ++q) {
       const int4 t = s_items[q];
       if (t.x < 0) break;
@@ -115,6 +118,8 @@ __device__ __forceinline__ void ens_rhs(const EnsembleArgs& a, int set0, int nse
       ens_tile<MODE>(sr, t.y, t.z);
       __syncthreads();  // the tile is done with sr and the dynamic shared memory
     }
+    if (threadIdx.x == 0) s_next = nxt;
+    __syncthreads();
   }
 }
 
@@ -145,7 +150,8 @@ static __device__ __forceinline__ void ens_assemble(const EnsembleArgs& a, int k
     if (threadIdx.x < kChunk && b0 + (int)threadIdx.x < a.ncells)
       s_cells[threadIdx.x] = a.cells[b0 + threadIdx.x];  // the chunk's blocks at once
     __syncthreads();  // every thread has read s_next; the blocks are staged
-    if (threadIdx.x == 0) s_next = (int)atomicAdd(ctr, 1u) * kChunk;
+    int nxt = 0;  // the next chunk, published at this chunk's end
+    if (threadIdx.x == 0) nxt = (int)atomicAdd(ctr, 1u) * kChunk;
     const int b1 = b0 + kChunk < a.ncells ? b0 + kChunk : a.ncells;
     for (int b = b0; b < b1; ++b) {
       const int2 w = s_cells[b - b0];
@@ -176,6 +182,7 @@ static __device__ __forceinline__ void ens_assemble(const EnsembleArgs& a, int k
             assemble_cell<FAST, 4>(ad[q], false, c % ad[q].nx, c / ad[q].nx);
       }
     }
+    if (threadIdx.x == 0) s_next = nxt;
     __syncthreads();  // the chunk is done; s_next is visible
   }
 }

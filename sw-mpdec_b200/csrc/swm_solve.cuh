@@ -902,7 +902,10 @@ __device__ __forceinline__ bool jacobi_batch_solve(const JacobiBatchArgs& a, dou
           s_items[threadIdx.x] = make_int2(set * a.nprob + t.x, t.y);
         }
         __syncthreads();  // every thread has read s_next; the items are staged
-        if (threadIdx.x == 0) s_next = (int)atomicAdd(a.work, 1u) * kJacChunk;
+        // the next chunk, fetched now and published at this chunk's end, so that no
+        // thread waits for the atomic before the chunk's work
+        int nxt = 0;
+        if (threadIdx.x == 0) nxt = (int)atomicAdd(a.work, 1u) * kJacChunk;
         const int w1 = w0 + kJacChunk < nwork ? w0 + kJacChunk : nwork;
         for (int w = w0; w < w1; ++w) {
           const int2 it = s_items[w - w0];  // (system, tile)
@@ -918,6 +921,7 @@ __device__ __forceinline__ bool jacobi_batch_solve(const JacobiBatchArgs& a, dou
             since += kPerTile;
           }
         }
+        if (threadIdx.x == 0) s_next = nxt;
         __syncthreads();  // the chunk is done; s_next is visible
       }
       if (cur >= 0) flush();
