@@ -352,6 +352,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--ensemble-only", action="store_true")  # profiling runs
+    ap.add_argument("--ensemble-island", type=int, default=0)  # profiling: one island N^2
     ap.add_argument("--no-accuracy", action="store_true")  # profiling runs: no wet-dry leg
     ap.add_argument("--n", type=int, default=2048)
     # profiling runs only: a subset of the timed forms, or another time scheme (its
@@ -394,7 +395,9 @@ def main():
         # ensemble: 256 problems of uneven size in one batch (split; the step form and the
         # Jacobi sweeps per pass autotuned); under torchrun the problem list is sharded
         # across ranks
-        members = cases.ensemble(seed=0)
+        # profiling: a batch holding one island grid (the single-grid workload's systems)
+        members = ([cases.case("island", n=args.ensemble_island)] if args.ensemble_island
+                   else cases.ensemble(seed=0))
         sizes = [m["nx"] * m["ny"] for m in members]
         mine = replicas.shard(sizes, rank, world)
         plist = [swm.make_params(m["nx"], m["ny"], m["x0"], m["x1"], g=m["g"], cfl=m["cfl"],
@@ -444,8 +447,10 @@ def main():
             # launch by a global timer inside it, the per-phase form by CUDA events)
             restore()
             forms[name]["phase_ms"] = {k: round(v, 4) for k, v in bt.phase_times().items()}
-        ens = {"workload": "256 problems, sides log-uniform in [64,512], vortex / dam break / "
-                           "Gaussian lake families, seed 0, split precision",
+        ens = {"workload": (f"one island {args.ensemble_island}^2 problem, split precision"
+                            if args.ensemble_island else
+                            "256 problems, sides log-uniform in [64,512], vortex / dam break / "
+                            "Gaussian lake families, seed 0, split precision"),
                "value": cell_steps / (ms_ens * 1e-3), "unit": "cell-steps/s",
                "cells": int(sum(sizes)), "ms_per_step": ms_ens / args.steps,
                "schedule": {"form": "persistent" if launches == 1 else "phased",
