@@ -824,7 +824,8 @@ __device__ __forceinline__ bool jacobi_batch_solve(const JacobiBatchArgs& a, dou
   __shared__ unsigned long long s_acc[kMaxBlock + 1][3];
   __shared__ __align__(16) JacobiArgs sd;
   __shared__ int s_ok, s_cnt, s_p, s_active, s_Tp, s_first, s_cur, s_next;
-  __shared__ int2 s_items[kJacChunk];  // a chunk's (system, tile) items
+  __shared__ int2 s_items[2][kJacChunk];  // (system, tile) items of two chunks
+  __shared__ int s_claim[2];              // the chunk after the current one
   static_assert(sizeof(JacobiArgs) % 8 == 0 && sizeof(JacobiArgs) / 8 <= JNT, "descriptor copy");
   const int blk = a.block < 1 ? 1 : (a.block > TB ? TB : a.block);
   const int nsys = a.nsets * a.nprob, nwork = a.nsets * a.ntiles;
@@ -890,28 +891,38 @@ __device__ __forceinline__ bool jacobi_batch_solve(const JacobiBatchArgs& a, dou
   };
   for (;;) {
     if (a.work) {
-      // chunks of kJacChunk consecutive work items taken one ahead from the shared
-      // counter (dynamic balance), their items read in one round trip; a system stays
-      // staged, and its sums in the thread accumulators, while consecutive items
-      // belong to it
+      // chunks of kJacChunk consecutive work items claimed from the shared counter
+      // (dynamic balance) two ahead: while a chunk runs, the next chunk's items are
+      // read into registers and the chunk after it is claimed; both are published at
+      // the chunk's closing barrier, so no chunk waits on a global round trip.  A
+      // system stays staged, and its sums in the thread accumulators, while
+      // consecutive items belong to it.
+      auto item = [&](int w) {  // (system, tile) of work item w < nwork
+        const int set = w / a.ntiles;
+        const int2 t = a.tiles[w - set * a.ntiles];
+        return make_int2(set * a.nprob + t.x, t.y);
+      };
       __syncthreads();
-      if (threadIdx.x == 0) s_next = (int)atomicAdd(a.work, 1u) * kJacChunk;
+      if (threadIdx.x == 0) {
+        s_next = (int)atomicAdd(a.work, 1u) * kJacChunk;
+        s_claim[0] = (int)atomicAdd(a.work, 1u) * kJacChunk;
+      }
       __syncthreads();
-      int cur = -1, since = 0;
-      for (int w0 = s_next; w0 < nwork; w0 = s_next) {
-        if (threadIdx.x < kJacChunk && w0 + (int)threadIdx.x < nwork) {
-          const int w = w0 + threadIdx.x, set = w / a.ntiles;
-          const int2 t = a.tiles[w - set * a.ntiles];
-          s_items[threadIdx.x] = make_int2(set * a.nprob + t.x, t.y);
-        }
-        __syncthreads();  // every thread has read s_next; the items are staged
-        // the next chunk, fetched now and published at this chunk's end, so that no
-        // thread waits for the atomic before the chunk's work
-        int nxt = 0;
+      if (threadIdx.x < kJacChunk && s_next + (int)threadIdx.x < nwork)
+        s_items[0][threadIdx.x] = item(s_next + threadIdx.x);
+      int cur = -1, since = 0, buf = 0;
+      int w0 = s_next;
+      __syncthreads();
+      while (w0 < nwork) {
+        const int wn = s_claim[buf];  // the next chunk
+        int2 pre = make_int2(0, 0);   // its items, in flight while this chunk runs
+        if (threadIdx.x < kJacChunk && wn + (int)threadIdx.x < nwork)
+          pre = item(wn + threadIdx.x);
+        int nxt = 0;  // the chunk after it
         if (threadIdx.x == 0) nxt = (int)atomicAdd(a.work, 1u) * kJacChunk;
         const int w1 = w0 + kJacChunk < nwork ? w0 + kJacChunk : nwork;
         for (int w = w0; w < w1; ++w) {
-          const int2 it = s_items[w - w0];  // (system, tile)
+          const int2 it = s_items[buf][w - w0];  // (system, tile)
           const int sys = it.x;
           if (sys != cur || since + kPerTile > kAccFlushCells) {
             if (cur >= 0) flush();
@@ -924,8 +935,11 @@ __device__ __forceinline__ bool jacobi_batch_solve(const JacobiBatchArgs& a, dou
             since += kPerTile;
           }
         }
-        if (threadIdx.x == 0) s_next = nxt;
-        __syncthreads();  // the chunk is done; s_next is visible
+        if (threadIdx.x < kJacChunk) s_items[buf ^ 1][threadIdx.x] = pre;
+        if (threadIdx.x == 0) s_claim[buf ^ 1] = nxt;
+        __syncthreads();  // the chunk is done; the next one's items and claim are visible
+        buf ^= 1;
+        w0 = wn;
       }
       if (cur >= 0) flush();
     } else {
