@@ -126,11 +126,11 @@ struct JacBatchState {
   int Tp;        // sweeps of the coming pass
   int rollback;  // the coming pass redoes the last one with Tp sweeps
   int first;     // the coming pass is the first (initial residual checked)
-  int cur;       // buffer holding x^k: 0 = b, 1 = xa, 2 = xb
-  int result;    // final iterate: 0 = zero vector, 1 = xa, 2 = xb
+  int cur;       // buffer holding x^k: 0 = b, 1 = xa, 2 = xb, 3 = the destination
+  int result;    // final iterate: 0 = zero vector, 1 = xa, 2 = xb, 3 = the destination
   int final_k;
   int maxhit;
-  int pad;
+  int xnext;     // buffer the coming pass writes: 1 = xa, 2 = xb, 3 = the destination
   double r_prev;  // residual sum of the last sweep of the previous pass (pass planning)
   unsigned long long acc[kMaxBlock + 1][3];
 };

@@ -732,8 +732,6 @@ __device__ void stencil_tiles(const JacobiArgs& a, const double* xin, double* xo
 // applies the single-problem stop rule to every problem (stop, redo the pass with
 // fewer sweeps, or continue), and a second barrier publishes the decisions.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ int xout_id(int cur) { return cur == 1 ? 2 : 1; }
-
 // CTA 0: the stop rule of jacobi_iteration.f90:71-81 for every active system.
 static __device__ void batch_decide(const JacobiBatchArgs& a, int blk, int* s_cnt) {
   if (threadIdx.x == 0) *s_cnt = 0;
@@ -744,12 +742,13 @@ static __device__ void batch_decide(const JacobiBatchArgs& a, int blk, int* s_cn
     JacBatchState* S = &a.st[p];
     if (!__ldcg(&S->active)) continue;
     const JacobiArgs& d = a.descs[p];
-    int k = __ldcg(&S->k), Tp = __ldcg(&S->Tp), cur = __ldcg(&S->cur);
+    int k = __ldcg(&S->k), Tp = __ldcg(&S->Tp);
+    const int xnext = __ldcg(&S->xnext);  // the buffer the pass just wrote
     const int first = __ldcg(&S->first), rollback = __ldcg(&S->rollback);
     int act = 1;
     if (rollback) {  // the redone pass delivered x^{final_k}
       act = 0;
-      S->result = xout_id(cur);
+      S->result = xnext;
     } else {
       int stop = -1;
       if (first && limbs_le(__ldcg(&S->acc[0][0]), __ldcg(&S->acc[0][1]),
@@ -775,7 +774,7 @@ static __device__ void batch_decide(const JacobiBatchArgs& a, int blk, int* s_cn
           S->Tp = stop;
         } else {
           act = 0;
-          S->result = xout_id(cur);
+          S->result = xnext;
         }
       } else {
         k += Tp;
@@ -784,9 +783,9 @@ static __device__ void batch_decide(const JacobiBatchArgs& a, int blk, int* s_cn
           act = 0;
           S->maxhit = 1;
           S->final_k = k;
-          S->result = xout_id(cur);
+          S->result = xnext;
         } else {
-          S->cur = xout_id(cur);
+          S->cur = xnext;
           const double rT = limbs_value(__ldcg(&S->acc[Tp][0]), __ldcg(&S->acc[Tp][1]),
                                         __ldcg(&S->acc[Tp][2]));
           const double rP = Tp >= 2 ? limbs_value(__ldcg(&S->acc[Tp - 1][0]),
@@ -794,9 +793,18 @@ static __device__ void batch_decide(const JacobiBatchArgs& a, int blk, int* s_cn
                                                   __ldcg(&S->acc[Tp - 1][2]))
                                     : __ldcg(&S->r_prev);
           S->r_prev = rT;
-          const int plan =
-              plan_sweeps(rT, rP, limbs_value(d.thresh[0], d.thresh[1], d.thresh[2]), blk);
+          const double th = limbs_value(d.thresh[0], d.thresh[1], d.thresh[2]);
+          const int plan = plan_sweeps(rT, rP, th, blk);
           S->Tp = (d.maxiter - k < plan) ? d.maxiter - k : plan;
+          // the next pass writes the other ping-pong buffer or, when it is expected to
+          // be the last, the destination itself (not the rhs, not the pass's input, and
+          // only with unpadded rows), which saves copying the result there
+          const bool expect_stop = rP > 0. && rT > 0. && rT < rP && th > 0. &&
+                                   log(th / rT) / log(rT / rP) <= (double)blk;
+          const int pitch = d.pitch > 0 ? d.pitch : d.nx;
+          S->xnext = (expect_stop && pitch == d.nx && d.out != d.b && xnext != 3)
+                         ? 3
+                         : (xnext == 1 ? 2 : 1);
         }
       }
     }
@@ -823,7 +831,7 @@ template <int TB, bool RECIP>
 __device__ __forceinline__ bool jacobi_batch_solve(const JacobiBatchArgs& a, double* jsm) {
   __shared__ unsigned long long s_acc[kMaxBlock + 1][3];
   __shared__ __align__(16) JacobiArgs sd;
-  __shared__ int s_ok, s_cnt, s_p, s_active, s_Tp, s_first, s_cur, s_next;
+  __shared__ int s_ok, s_cnt, s_p, s_active, s_Tp, s_first, s_cur, s_xnext, s_next;
   __shared__ int2 s_items[2][kJacChunk];  // (system, tile) items of two chunks
   __shared__ int s_claim[2];              // the chunk after the current one
   static_assert(sizeof(JacobiArgs) % 8 == 0 && sizeof(JacobiArgs) / 8 <= JNT, "descriptor copy");
@@ -839,6 +847,7 @@ __device__ __forceinline__ bool jacobi_batch_solve(const JacobiBatchArgs& a, dou
     S->rollback = 0;
     S->first = 1;
     S->cur = 0;
+    S->xnext = 1;
     S->result = 0;
     S->final_k = 0;
     S->maxhit = 0;
@@ -874,6 +883,7 @@ __device__ __forceinline__ bool jacobi_batch_solve(const JacobiBatchArgs& a, dou
       s_Tp = __ldcg(&S->Tp);
       s_first = __ldcg(&S->first);
       s_cur = __ldcg(&S->cur);
+      s_xnext = __ldcg(&S->xnext);
     }
     if (sys != loaded) {
       if (threadIdx.x < sizeof(JacobiArgs) / 8)
@@ -885,8 +895,8 @@ __device__ __forceinline__ bool jacobi_batch_solve(const JacobiBatchArgs& a, dou
     __syncthreads();
   };
   auto tile = [&](int t) {
-    const double* xin = s_cur == 0 ? sd.b : (s_cur == 1 ? sd.xa : sd.xb);
-    double* xout = s_cur == 1 ? sd.xb : sd.xa;
+    const double* xin = s_cur == 0 ? sd.b : (s_cur == 1 ? sd.xa : (s_cur == 2 ? sd.xb : sd.out));
+    double* xout = s_xnext == 1 ? sd.xa : (s_xnext == 2 ? sd.xb : sd.out);
     stencil_tiles<TB, RECIP, true>(sd, xin, xout, s_Tp, s_first != 0, acc, jsm, t, s_acc);
   };
   for (;;) {
@@ -964,10 +974,12 @@ __device__ __forceinline__ bool jacobi_batch_solve(const JacobiBatchArgs& a, dou
     __syncthreads();
     if (s_cnt == 0) break;
   }
-  // deliver every system's final iterate (haVec) to its destination
+  // deliver every system's final iterate (haVec) to its destination, unless the last
+  // pass wrote it there
   for (int p = 0; p < nsys; ++p) {
     const JacobiArgs& d = a.descs[p];
     const int res = __ldcg(&a.st[p].result);
+    if (res == 3) continue;
     const double* src = res == 1 ? d.xa : d.xb;
     const int n = d.nx * d.ny, pitch = d.pitch > 0 ? d.pitch : d.nx;
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
