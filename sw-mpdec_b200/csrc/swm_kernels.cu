@@ -586,7 +586,23 @@ __global__ void __launch_bounds__(128)
     ly = dmax(ly, __shfl_down_sync(0xffffffffu, ly, o));
   }
   b = __any_sync(0xffffffffu, b);
+  // block maxima first: one pair of atomics per block, not per warp (the atomics of a
+  // problem's blocks all go to the same two words)
+  __shared__ double s_lx[4], s_ly[4];
+  __shared__ int s_b[4];
+  static_assert(128 / 32 == 4, "four warps per block");
   if ((threadIdx.x & 31) == 0) {
+    s_lx[threadIdx.x >> 5] = lx;
+    s_ly[threadIdx.x >> 5] = ly;
+    s_b[threadIdx.x >> 5] = b;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int q = 1; q < 4; ++q) {
+      lx = dmax(lx, s_lx[q]);
+      ly = dmax(ly, s_ly[q]);
+      b |= s_b[q];
+    }
     atomicMax(&lam[2 * w.x], (unsigned long long)__double_as_longlong(lx));
     atomicMax(&lam[2 * w.x + 1], (unsigned long long)__double_as_longlong(ly));
     if (b) atomicOr(&bad[w.x], 1);
